@@ -1,0 +1,358 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 G1 step on the randomised 65,536-env workload.
+
+Workload (per GPU): 65,536 envs, dt = 2 ms, decimation 10, 1,000 substeps
+(100 policy steps) per bench step; PD targets stand + U(-0.3, 0.3) x range
+redrawn on the device each policy step; per-env friction U[0.4, 1.0] and
+base-mass offset U[-1, +3] kg; initial base height U[0.75, 0.85] m; envs
+reset in the kernel when the base height drops below 0.3 m.  A bench step
+replays one CUDA graph holding the 100 policy-step launches (state goes
+through HBM between policy steps, as in an RL loop).
+
+Metric: env-steps/s, one env-step = one physics substep of one env (the
+reference's nenv * nsteps * nsub, src/g1_kernel.cu:238).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own 65,536
+envs (independent replicas, no collective on the data path); the timed
+region is bracketed by barriers and the max over ranks is reported.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic work per env-substep (FP32 flops, FMA = 2): the reference
+# algorithm's counted add/sub/mul with its per-step recomputation of constant
+# tree rotations, spatial inertias and hinge S vectors removed.
+FLOPS_PER_ENV_STEP = 36600.0
+# Algorithmic bytes per env per launch: SoA state in (qpos 36, qvel 35,
+# anchor 16, ctrl 29, mu, dmass) and out (qpos, qvel, anchor, ctrl), float32.
+BYTES_PER_ENV_LAUNCH = 4.0 * ((36 + 35 + 16 + 29 + 2) + (36 + 35 + 16 + 29))
+
+NENV = 65536
+SUBSTEPS = 1000
+DECIM = 10
+DT = 2e-3
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nenv", type=int, default=NENV)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# -------------------------------------------------------- CPU baseline
+def cpu_reference(seconds, nenv):
+    """The reference's own FP32 step (oracle/_ref/g1ref_rollout, built from
+    the reference sources) on this host's cores: a bounded sample of the
+    workload, all hardware threads."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "g1ref_rollout")
+    if not os.path.exists(exe):
+        return None
+    threads = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread")
+    out = subprocess.run([exe, "--nenv", str(nenv), "--steps", str(SUBSTEPS), "--decim", str(DECIM),
+                          "--seconds", str(seconds), "--threads", str(threads)],
+                         capture_output=True, text=True, env=env, timeout=seconds * 10 + 120)
+    if out.returncode != 0:
+        return None
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    return {"value": r["env_steps_per_s"], "unit": "env-steps/s", "cores": r["threads"], "kind": "reference",
+            "sample": (f"first {r['envs']} of the {nenv} envs x {r['substeps']} substeps (dt 2 ms, decimation "
+                       f"10, target redraw, reset at z<0.3; nominal friction/mass: the reference has no "
+                       f"per-env parameters), reference g1_step FP32 via OpenMP, {r['seconds']:.1f} s")}
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    ws = []
+    res = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference(4.0, args.nenv)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/g1ref_rollout is not built "
+                                                                  "(make -C oracle ref needs the reference sources)"}))
+            return 0
+        if i >= args.warmup:
+            ws.append(r["value"])
+            res = r
+    v = statistics.mean(ws)
+    line = {"impl": "reference", "metric": "env-steps/s", "value": v, "unit": "env-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"randomised plain step, {args.nenv} envs, dt 2 ms, decimation 10, "
+                                   f"{SUBSTEPS} substeps", "envs": args.nenv, "substeps": SUBSTEPS,
+                       "decimation": DECIM, "dt": DT},
+            "cpu_baseline": {"value": v, "unit": "env-steps/s", "cores": res["cores"], "kind": "reference",
+                             "sample": res["sample"]},
+            "e2e": {"value": v, "unit": "env-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------- our arm
+def ours(args, world, rank, local):
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+
+    from g1sim_b200 import _lib, workloads
+    from g1sim_b200 import g1sim as G
+    L = _lib.lib()
+
+    n = args.nenv
+    w = workloads.randomized(nenv=n, seed=rank)
+    f32 = dict(dtype=torch.float32, device=device)
+    init = {k: torch.tensor(w[k], **f32) for k in ("qpos", "qvel", "anchor", "ctrl", "mu", "dmass")}
+    st = {k: init[k].clone() for k in ("qpos", "qvel", "anchor", "ctrl")}
+    rc = torch.zeros(n, dtype=torch.int32, device=device)
+    cfg = _lib.default_config(dt=DT)
+    npolicy = SUBSTEPS // DECIM
+    stream = torch.cuda.Stream(device)
+
+    def launch_policy_step(k):
+        G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 1, DECIM, config=cfg, seed=rank,
+                  step0=k, mu=init["mu"], dmass=init["dmass"], reset_count=rc)
+
+    def reset_state():
+        for k in st:
+            st[k].copy_(init[k])
+
+    # capture the 100 policy-step launches in one CUDA graph
+    with torch.cuda.stream(stream):
+        reset_state()
+        launch_policy_step(0)  # one eager launch before capture (kernel attributes, lazy loading)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for k in range(npolicy):
+                launch_policy_step(k)
+    launches_per_step = npolicy
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > 126 MB L2
+
+    def timed_steps(count):
+        times = []
+        for _ in range(count):
+            with torch.cuda.stream(stream):
+                reset_state()
+                flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                graph.replay()
+                e1.record(stream)
+            stream.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times
+
+    timed_steps(args.warmup)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        times = timed_steps(args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(statistics.mean(times), world, device)
+    env_steps = float(n) * SUBSTEPS
+    value = env_steps * world / (ms * 1e-3)
+
+    # ---- kernel-level roofline (dominant kernel: one policy-step launch)
+    launch_ms = ms / launches_per_step
+    flops_launch = FLOPS_PER_ENV_STEP * n * DECIM
+    achieved_tf = flops_launch / (launch_ms * 1e-3) / 1e12
+    ffma_tf = C.c_float()
+    ffma_ms = C.c_float()
+    _lib.check(L.g1b_ffma_peak(20000, C.byref(ffma_tf), C.byref(ffma_ms)), "g1b_ffma_peak")
+    peak_tf = float(ffma_tf.value)
+    hbm_gbs = BYTES_PER_ENV_LAUNCH * n / (launch_ms * 1e-3) / 1e9
+
+    # ---- single-launch (fully persistent) variant, reported alongside
+    with torch.cuda.stream(stream):
+        reset_state()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], npolicy, DECIM, config=cfg, seed=rank,
+                  step0=0, mu=init["mu"], dmass=init["dmass"], reset_count=rc)
+        e1.record(stream)
+    stream.synchronize()
+    single_ms = e0.elapsed_time(e1)
+
+    # ---- end to end through the public API, host buffers in pinned memory
+    host_in = {k: init[k].cpu().pin_memory() for k in init}
+    host_out = {k: torch.empty_like(host_in[k]).pin_memory() for k in ("qpos", "qvel", "anchor", "ctrl")}
+    dev_in = {k: torch.empty_like(init[k]) for k in init}
+    h2d = sum(t.numel() * 4 for t in host_in.values())
+    d2h = sum(t.numel() * 4 for t in host_out.values())
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for k in host_in:
+                dev_in[k].copy_(host_in[k], non_blocking=True)
+            for k in range(npolicy):
+                G.rollout(dev_in["qpos"], dev_in["qvel"], dev_in["anchor"], dev_in["ctrl"], 1, DECIM, config=cfg,
+                          seed=rank, step0=k, mu=dev_in["mu"], dmass=dev_in["dmass"])
+            for k in host_out:
+                host_out[k].copy_(dev_in[k], non_blocking=True)
+        stream.synchronize()
+
+    e2e_step()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world, device)
+    e2e_value = env_steps * world / e2e_s
+
+    resets = int(rc.sum().item())
+    finite = bool(torch.isfinite(st["qpos"]).all().item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference(args.cpu_seconds, n)
+
+    if rank == 0:
+        line = {
+            "metric": "env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"randomised plain step, {n} envs per GPU, dt 2 ms, decimation 10, "
+                                   f"{SUBSTEPS} substeps per step (CUDA graph of {npolicy} policy-step launches)",
+                       "envs_per_gpu": n, "substeps": SUBSTEPS, "decimation": DECIM, "dt": DT,
+                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
+            "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                         "frac": achieved_tf / peak_tf if peak_tf > 0 else None, "traffic": None,
+                         "peak_source": "measured FFMA microbenchmark (g1b_ffma_peak), this run",
+                         "flops_per_env_step": FLOPS_PER_ENV_STEP, "kernel": "rollout_kernel, 1 policy step",
+                         "kernel_ms": launch_ms, "hbm_gbs": hbm_gbs},
+            "e2e": {"value": e2e_value, "unit": "env-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+            "single_launch": {"value": env_steps / (single_ms * 1e-3), "ms": single_ms},
+            "resets_last_step": resets, "finite": finite,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        del graph
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+    return ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,72 @@
+"""ctypes binding of libg1cuda.so (the C-ABI declared in include/g1sim_b200.h).
+
+The library is the only compute path: if it is missing, or no CUDA device is
+present, every entry point raises -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+from .build import LIB
+
+_lib = None
+
+
+class Config(C.Structure):
+    """g1b_config (mirrors the reference G1Config, src/g1_types.h:33-42)."""
+    _fields_ = [(n, C.c_float) for n in (
+        "gravity_z", "contact_kn", "contact_dn", "contact_kt", "contact_dt",
+        "limit_kp", "limit_kd", "dt")]
+
+
+class RolloutParams(C.Structure):
+    """g1b_rollout_params."""
+    _fields_ = [("seed", C.c_uint), ("step0", C.c_int), ("target_frac", C.c_float),
+                ("reset_z", C.c_float), ("z0_lo", C.c_float), ("z0_hi", C.c_float),
+                ("redraw", C.c_int)]
+
+
+_vp = C.c_void_p
+
+
+def lib():
+    """Load libg1cuda.so once and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise RuntimeError(f"{LIB} is missing: build it with `python -m g1sim_b200.build` "
+                           "(nvcc, sm_100a); there is no CPU fallback")
+    L = C.CDLL(LIB)
+    L.g1_cuda_step.argtypes = [C.c_int, C.c_int] + [_vp] * 8
+    L.g1_cuda_step.restype = None
+    L.g1_cuda_reset_done.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_uint, C.c_float, C.c_float, _vp]
+    L.g1_cuda_reset_done.restype = None
+    L.g1b_sizes.argtypes = [C.POINTER(C.c_int)] * 5
+    L.g1b_default_config.argtypes = [C.POINTER(Config)]
+    L.g1b_last_error.restype = C.c_char_p
+    L.g1b_step.argtypes = [C.c_int, C.c_int, C.POINTER(Config)] + [_vp] * 12
+    L.g1b_rollout.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(Config), C.POINTER(RolloutParams)] + [_vp] * 11
+    L.g1b_set_launch.argtypes = [C.c_int, C.c_int]
+    L.g1b_get_launch.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.g1b_autotune.argtypes = [C.c_int, C.c_int, _vp, C.POINTER(C.c_float)]
+    L.g1b_ffma_peak.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    _lib = L
+    return L
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = lib().g1b_last_error().decode(errors="replace")
+        raise RuntimeError(f"{what} failed ({rc}): {msg}")
+
+
+def default_config(dt=None):
+    c = Config()
+    check(lib().g1b_default_config(C.byref(c)), "g1b_default_config")
+    if dt is not None:
+        c.dt = dt
+    return c
+
+
+def last_error():
+    return lib().g1b_last_error().decode(errors="replace")

@@ -20,6 +20,7 @@ few compiler steps that the G1 needs in plain numpy:
 Outputs (both committed):
   g1sim_b200/model/g1_model_data.py   -- numpy-free Python literals
   g1sim_b200/csrc/g1_model_data.h     -- C/C++ constant tables (double)
+  g1sim_b200/csrc/g1_model_derived.h  -- derived tables for the device code
 
 Usage:  python g1sim_b200/model/gen_model.py <dir containing g1_stripped.xml and g1_raw.xml>
 """
@@ -280,6 +281,60 @@ def emit_h(data, path):
         f.write("\n#endif  // G1M_MODEL_DATA_H\n")
 
 
+def derived(data):
+    """Tables the device code uses directly (computed once, in double)."""
+    nb = data["NB"]
+    tree_rot, tree_ident, sp_inertia, axis_idx = [], [], [], []
+    for i in range(nb):
+        q = data["tree_quat"][i]
+        ident = q == [1.0, 0.0, 0.0, 0.0]
+        tree_ident.append(1 if ident else 0)
+        tree_rot.append(list(map(float, quat_to_mat(q).reshape(-1))))
+        m = data["mass"][i]
+        c = np.asarray(data["com"][i])
+        icom = np.asarray(data["inertia_com"][i]).reshape(3, 3)
+        cx = np.array([[0, -c[2], c[1]], [c[2], 0, -c[0]], [-c[1], c[0], 0]])
+        J = icom + m * cx @ cx.T          # about the body origin
+        H = m * cx                        # angular-linear block
+        # J (xx, yy, zz, xy, xz, yz), H row-major, M = m I
+        sp_inertia.append([J[0, 0], J[1, 1], J[2, 2], J[0, 1], J[0, 2], J[1, 2]]
+                          + list(H.reshape(-1)) + [m])
+    for h, ax in enumerate(data["jnt_axis"]):
+        nz = [k for k in range(3) if ax[k] != 0.0]
+        assert len(nz) == 1 and ax[nz[0]] == 1.0, "hinge axes must be +x, +y or +z"
+        assert data["jnt_anchor"][h] == [0.0, 0.0, 0.0], "hinge anchors must be at the body origin"
+        axis_idx.append(nz[0])
+    return dict(tree_rot=tree_rot, tree_ident=tree_ident, sp_inertia=sp_inertia,
+                axis_idx=axis_idx)
+
+
+def emit_derived_h(data, der, path):
+    def arr(name, rows, ctype="double"):
+        flat = []
+        for r in rows:
+            flat.extend(r if isinstance(r, (list, tuple)) else [r])
+        if ctype == "int":
+            body = ", ".join(str(int(x)) for x in flat)
+        else:
+            body = ",\n  ".join(", ".join(_fmt(x) for x in flat[i:i + 6])
+                                for i in range(0, len(flat), 6))
+        return f"G1M_TABLE {ctype} {name}[{len(flat)}] = {{\n  {body}\n}};\n"
+
+    with open(path, "w") as f:
+        f.write("// Generated by g1sim_b200/model/gen_model.py -- do not edit.\n")
+        f.write("// Derived G1 tables in double: tree rotation matrices (row-major, from\n")
+        f.write("// the unit tree quaternions), rigid-body spatial inertia about each body\n")
+        f.write("// origin as J(xx,yy,zz,xy,xz,yz), H = m [c]x (row-major), m, and the\n")
+        f.write("// hinge axis index (every axis is +x, +y or +z, every anchor is 0).\n")
+        f.write("#ifndef G1M_MODEL_DERIVED_H\n#define G1M_MODEL_DERIVED_H\n")
+        f.write('#include "g1_model_data.h"\n\n')
+        f.write(arr("g1m_tree_rot", der["tree_rot"]))
+        f.write(arr("g1m_tree_ident", der["tree_ident"], "int"))
+        f.write(arr("g1m_sp_inertia", der["sp_inertia"]))
+        f.write(arr("g1m_axis_idx", der["axis_idx"], "int"))
+        f.write("\n#endif  // G1M_MODEL_DERIVED_H\n")
+
+
 def main():
     model_dir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("G1_MJCF_DIR")
     if not model_dir:
@@ -287,6 +342,7 @@ def main():
     data = build(model_dir)
     emit_py(data, os.path.join(HERE, "g1_model_data.py"))
     emit_h(data, os.path.join(PKG, "csrc", "g1_model_data.h"))
+    emit_derived_h(data, derived(data), os.path.join(PKG, "csrc", "g1_model_derived.h"))
     print(f"NB={data['NB']} NV={data['NV']} NQ={data['NQ']} NU={data['NU']} NC={data['NC']}")
 
 

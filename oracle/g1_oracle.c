@@ -561,6 +561,71 @@ void g1o_step_soa(int nenv, int nsub, const g1o_config* cfg, double* qpos, doubl
   }
 }
 
+/* ------------------------------------------------------ branch margins --- */
+/* Distance of one substep from every branch of the discontinuous model,
+ * normalised by the size of FP32 rounding at that branch: contact touchdown
+ * (depth 0, 1e-6 m), normal-force clamps (0 and 500 N, 1e-2 N), stick/slip
+ * (|ft| = mu fn, 1e-2 N + 1e-6 relative), soft joint limits (1e-6 rad) and
+ * the servo torque clamp (1e-3 N m).  A value below 1 means an FP32 step may
+ * legitimately take the other branch (reference src/g1_core.h:129-150,
+ * :168-174). */
+static double branch_margin(const g1o_config* cfg, const g1o_envparams* ep, const double* qpos,
+                            const double* qvel, const double* ctrl, const double* anchor_in) {
+  ws_t w;
+  double anchor[2 * NC];
+  memcpy(anchor, anchor_in, sizeof(anchor));
+  fk_vel(qpos, qvel, &w);
+  double m = 1e300;
+#define MARGIN(x) do { double _x = (x); if (_x < m) m = _x; } while (0)
+  for (int k = 0; k < NC; ++k) {
+    int b = g1m_contact_body[k];
+    v3 r = ld3(g1m_contact_pos + 3 * k);
+    v3 p = add3(mv(&w.oR[b], r), w.oP[b]);
+    double depth = g1m_contact_radius - p.z;
+    MARGIN(fabs(depth) / 1e-6);
+    if (depth <= 0) continue;
+    v3 vp = mv(&w.oR[b], add3(w.v[b].l, crs3(w.v[b].a, r)));
+    double fn = cfg->contact_kn * depth - cfg->contact_dn * vp.z;
+    MARGIN(fabs(fn) / 1e-2);
+    MARGIN(fabs(fn - 500.0) / 1e-2);
+    if (fn < 0) fn = 0;
+    if (fn > 500.0) fn = 500.0;
+    double ax = anchor[2 * k] >= ANCHOR_FREE ? p.x : anchor[2 * k];
+    double ay = anchor[2 * k + 1] >= ANCHOR_FREE ? p.y : anchor[2 * k + 1];
+    double ftx = -cfg->contact_kt * (p.x - ax) - cfg->contact_dt * vp.x;
+    double fty = -cfg->contact_kt * (p.y - ay) - cfg->contact_dt * vp.y;
+    double ftn = sqrt(ftx * ftx + fty * fty), fmax = ep->mu * fn;
+    MARGIN(fabs(ftn - fmax) / (1e-2 + 1e-6 * (ftn > fmax ? ftn : fmax)));
+  }
+  for (int h = 0; h < NJ; ++h) {
+    double q = qpos[7 + h], qd = qvel[6 + h];
+    MARGIN(fabs(q - g1m_jnt_range[2 * h]) / 1e-6);
+    MARGIN(fabs(q - g1m_jnt_range[2 * h + 1]) / 1e-6);
+    double kp = g1m_act_kp[h] * ep->kp_scale, kv = g1m_act_kv[h] * ep->kd_scale;
+    double t = kp * (ctrl[h] - q) - kv * qd;
+    MARGIN(fabs(fabs(t) - g1m_act_frclim[h]) / 1e-3);
+  }
+#undef MARGIN
+  return m;
+}
+
+void g1o_branch_margin_soa(int nenv, const g1o_config* cfg, const double* qpos,
+                           const double* qvel, const double* anchor, const double* ctrl,
+                           const double* mu, const double* dmass, double* margin) {
+  size_t n = (size_t)nenv;
+  for (int e = 0; e < nenv; ++e) {
+    double qp[NQ], qv[NV], ct[NU], an[2 * NC];
+    for (int i = 0; i < NQ; ++i) qp[i] = qpos[i * n + e];
+    for (int i = 0; i < NV; ++i) qv[i] = qvel[i * n + e];
+    for (int i = 0; i < NU; ++i) ct[i] = ctrl[i * n + e];
+    for (int i = 0; i < 2 * NC; ++i) an[i] = anchor[i * n + e];
+    g1o_envparams ep = kDefaultEp;
+    if (mu) ep.mu = mu[e];
+    if (dmass) ep.dmass = dmass[e];
+    margin[e] = branch_margin(cfg, &ep, qp, qv, ct, an);
+  }
+}
+
 /* --------------------------------------------------------- RNG, reset --- */
 /* 32-bit xorshift-multiply integer hash (C. Wellons' "lowbias32"), the
  * reference's g1_hash (src/g1_kernel.cu:54-58). */

