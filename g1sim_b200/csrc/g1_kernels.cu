@@ -26,9 +26,12 @@
 namespace g1b {
 
 // ------------------------------------------------------------ scratch
+// volatile: the compiler must not forward a stored value to its later load
+// (same thread, same address), which would turn the whole scratch back into
+// long-lived registers and spill them.
 template <int BLOCK>
 struct SmemScratch {
-  float* p;
+  volatile float* p;
   template <int K>
   __host__ __device__ __forceinline__ float get() const { return p[K * BLOCK]; }
   template <int K>
@@ -68,12 +71,9 @@ __device__ __forceinline__ void load_state(const StateArgs& a, int e, EnvState& 
   for (int k = 0; k < 3; ++k) st.wb[k] = a.qvel[(3 + k) * n + e];
 #pragma unroll
   for (int k = 0; k < kNJ; ++k) st.qd[k] = a.qvel[(6 + k) * n + e];
-#pragma unroll
-  for (int k = 0; k < 2 * kNC; ++k) st.anchor[k] = a.anchor[k * n + e];
 }
 
-__device__ __forceinline__ void store_state(const StateArgs& a, int e, const EnvState& st,
-                                            const StepOut& out, bool has_out) {
+__device__ __forceinline__ void store_state(const StateArgs& a, int e, const EnvState& st) {
   const size_t n = (size_t)a.nenv;
 #pragma unroll
   for (int k = 0; k < 3; ++k) a.qpos[k * n + e] = st.pos[k];
@@ -87,22 +87,18 @@ __device__ __forceinline__ void store_state(const StateArgs& a, int e, const Env
   for (int k = 0; k < 3; ++k) a.qvel[(3 + k) * n + e] = st.wb[k];
 #pragma unroll
   for (int k = 0; k < kNJ; ++k) a.qvel[(6 + k) * n + e] = st.qd[k];
-#pragma unroll
-  for (int k = 0; k < 2 * kNC; ++k) a.anchor[k * n + e] = st.anchor[k];
-  if (has_out) {
-    if (a.foot_pos) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) a.foot_pos[k * n + e] = out.foot_pos[k];
-    }
-    if (a.foot_vel) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) a.foot_vel[k * n + e] = out.foot_vel[k];
-    }
-    if (a.cf) {
-#pragma unroll
-      for (int k = 0; k < kNC; ++k) a.cf[k * n + e] = out.fn[k];
-    }
-  }
+}
+
+// The env's in-memory arrays (ctrl, anchors, outputs), offset to env e.
+__device__ __forceinline__ EnvIO env_io(const StateArgs& a, const float* ctrl, int e) {
+  EnvIO io;
+  io.ctrl = ctrl + e;
+  io.anchor = a.anchor + e;
+  io.foot_pos = a.foot_pos ? a.foot_pos + e : nullptr;
+  io.foot_vel = a.foot_vel ? a.foot_vel + e : nullptr;
+  io.cf = a.cf ? a.cf + e : nullptr;
+  io.stride = (size_t)a.nenv;
+  return io;
 }
 
 __device__ __forceinline__ EnvParams load_params(const StateArgs& a, int e) {
@@ -125,13 +121,10 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(StateArgs a, const float* _
   for (int e = blockIdx.x * BLOCK + threadIdx.x; e < n; e += gridDim.x * BLOCK) {
     EnvState st;
     load_state(a, e, st);
-    float ct[kNU];
-#pragma unroll
-    for (int k = 0; k < kNU; ++k) ct[k] = __ldg(ctrl + (size_t)k * n + e);
+    const EnvIO io = env_io(a, ctrl, e);
     const EnvParams ep = load_params(a, e);
-    StepOut out;
-    for (int s = 0; s < nsub; ++s) step(st, ct, ep, cfg, scr, out);
-    store_state(a, e, st, out, nsub > 0);
+    for (int s = 0; s < nsub; ++s) step(st, io, ep, cfg, scr, s == nsub - 1);
+    store_state(a, e, st);
   }
 }
 
@@ -170,14 +163,16 @@ __device__ __forceinline__ float draw_target(unsigned seed, int e, int step, flo
   const float span = __fmul_rn(frac, __fsub_rn(hi, lo));
   return __fadd_rn(stand, __fmul_rn(r, span));
 }
+// writes the env's targets into its ctrl column (read back by the substeps)
 template <int J>
-__device__ __forceinline__ void draw_targets(float* ct, unsigned seed, int e, int step, float frac) {
-  ct[J] = draw_target<J>(seed, e, step, frac);
-  if constexpr (J + 1 < kNU) draw_targets<J + 1>(ct, seed, e, step, frac);
+__device__ __forceinline__ void draw_targets(float* ct, size_t stride, unsigned seed, int e, int step,
+                                             float frac) {
+  ct[J * stride] = draw_target<J>(seed, e, step, frac);
+  if constexpr (J + 1 < kNU) draw_targets<J + 1>(ct, stride, seed, e, step, frac);
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* __restrict__ ctrl,
+__global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* ctrl,
                                                         int* __restrict__ reset_count, int npolicy,
                                                         int decim, StepConfig cfg, RolloutParams rp) {
   extern __shared__ float sm[];
@@ -186,16 +181,13 @@ __global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* __re
   for (int e = blockIdx.x * BLOCK + threadIdx.x; e < n; e += gridDim.x * BLOCK) {
     EnvState st;
     load_state(a, e, st);
-    float ct[kNU];
-#pragma unroll
-    for (int k = 0; k < kNU; ++k) ct[k] = ctrl[(size_t)k * n + e];
+    const EnvIO io = env_io(a, ctrl, e);
     const EnvParams ep = load_params(a, e);
-    StepOut out;
     int resets = 0;
     for (int k = 0; k < npolicy; ++k) {
       const int stp = rp.step0 + k;
-      if (rp.redraw) draw_targets<0>(ct, rp.seed, e, stp, rp.target_frac);
-      for (int s = 0; s < decim; ++s) step(st, ct, ep, cfg, scr, out);
+      if (rp.redraw) draw_targets<0>(ctrl + e, (size_t)n, rp.seed, e, stp, rp.target_frac);
+      for (int s = 0; s < decim; ++s) step(st, io, ep, cfg, scr, k == npolicy - 1 && s == decim - 1);
       if (st.pos[2] < rp.reset_z) {
         const float u = uniform24(rp.seed ^ 0x5bd1e995u, (unsigned)e, (unsigned)stp);
         const float z0 = __fadd_rn(rp.z0_lo, __fmul_rn(u, __fsub_rn(rp.z0_hi, rp.z0_lo)));
@@ -211,13 +203,11 @@ __global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* __re
 #pragma unroll
         for (int i = 0; i < kNJ; ++i) st.qd[i] = 0.0f;
 #pragma unroll
-        for (int i = 0; i < 2 * kNC; ++i) st.anchor[i] = kAnchorFree;
+        for (int i = 0; i < 2 * kNC; ++i) a.anchor[(size_t)i * n + e] = kAnchorFree;
         ++resets;
       }
     }
-    store_state(a, e, st, out, npolicy > 0 && decim > 0);
-#pragma unroll
-    for (int k = 0; k < kNU; ++k) ctrl[(size_t)k * n + e] = ct[k];
+    store_state(a, e, st);
     if (reset_count) reset_count[e] += resets;
   }
 }

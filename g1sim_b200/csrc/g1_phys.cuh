@@ -69,6 +69,7 @@ struct FTab {
 template <int N>
 constexpr FTab<N> ftab(const double* src) {
   FTab<N> t{};
+#pragma unroll
   for (int i = 0; i < N; ++i) t.v[i] = (float)src[i];
   return t;
 }
@@ -204,11 +205,13 @@ template <int AX>
 G1_HD M3 rotA_gen(const M3& H, float c, float s) {
   constexpr int i = (AX + 1) % 3, j = (AX + 2) % 3;
   M3 B = H;  // B = A H: rows
+#pragma unroll
   for (int col = 0; col < 3; ++col) {
     B.m[3 * i + col] = c * H.m[3 * i + col] - s * H.m[3 * j + col];
     B.m[3 * j + col] = s * H.m[3 * i + col] + c * H.m[3 * j + col];
   }
   M3 r = B;  // r = B A^T: columns
+#pragma unroll
   for (int row = 0; row < 3; ++row) {
     r.m[3 * row + i] = c * B.m[3 * row + i] - s * B.m[3 * row + j];
     r.m[3 * row + j] = s * B.m[3 * row + i] + c * B.m[3 * row + j];
@@ -223,6 +226,7 @@ G1_HD V3 rotT(const V3& x) {
     return x;
   } else {
     V3 r;
+#pragma unroll
     for (int a = 0; a < 3; ++a)
       r.v[a] = tree_rot(I, a, 0) * x.v[0] + tree_rot(I, a, 1) * x.v[1] + tree_rot(I, a, 2) * x.v[2];
     return r;
@@ -234,6 +238,7 @@ G1_HD V3 rotTT(const V3& x) {
     return x;
   } else {
     V3 r;
+#pragma unroll
     for (int a = 0; a < 3; ++a)
       r.v[a] = tree_rot(I, 0, a) * x.v[0] + tree_rot(I, 1, a) * x.v[1] + tree_rot(I, 2, a) * x.v[2];
     return r;
@@ -245,15 +250,21 @@ G1_HD S3 rotT_sym(const S3& S) {
     return S;
   } else {
     float F[9];
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = 0; b < 3; ++b)
         F[3 * a + b] = S.s[sidx(a, b)];
     float B[9];
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = 0; b < 3; ++b)
         B[3 * a + b] = tree_rot(I, a, 0) * F[b] + tree_rot(I, a, 1) * F[3 + b] + tree_rot(I, a, 2) * F[6 + b];
     S3 r;
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = a; b < 3; ++b)
         r.s[sidx(a, b)] = B[3 * a + 0] * tree_rot(I, b, 0) + B[3 * a + 1] * tree_rot(I, b, 1) +
                           B[3 * a + 2] * tree_rot(I, b, 2);
@@ -266,11 +277,15 @@ G1_HD M3 rotT_gen(const M3& H) {
     return H;
   } else {
     float B[9];
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = 0; b < 3; ++b)
         B[3 * a + b] = tree_rot(I, a, 0) * H.m[b] + tree_rot(I, a, 1) * H.m[3 + b] + tree_rot(I, a, 2) * H.m[6 + b];
     M3 r;
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = 0; b < 3; ++b)
         r.m[3 * a + b] = B[3 * a + 0] * tree_rot(I, b, 0) + B[3 * a + 1] * tree_rot(I, b, 1) +
                          B[3 * a + 2] * tree_rot(I, b, 2);
@@ -302,7 +317,9 @@ G1_CONSTEVAL bool p_zero() {
 template <int I>
 G1_HD AI body_inertia() {
   AI r;
+#pragma unroll
   for (int k = 0; k < 6; ++k) r.J.s[k] = spi(I, k);
+#pragma unroll
   for (int k = 0; k < 9; ++k) r.H.m[k] = spi(I, 6 + k);
   const float m = spi(I, 15);
   r.M.s[0] = r.M.s[1] = r.M.s[2] = m;
@@ -339,6 +356,7 @@ G1_HD AI pelvis_inertia(float dmass) {
 // I v for a spatial inertia
 G1_HD SV ai_mul(const AI& I, const SV& x) {
   SV r;
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
     r.a.v[a] = I.J.s[sidx(a, 0)] * x.a.v[0] + I.J.s[sidx(a, 1)] * x.a.v[1] + I.J.s[sidx(a, 2)] * x.a.v[2] +
                I.H.m[3 * a + 0] * x.l.v[0] + I.H.m[3 * a + 1] * x.l.v[1] + I.H.m[3 * a + 2] * x.l.v[2];
@@ -378,13 +396,20 @@ G1_CONSTEVAL int slot() { return (I - 1) * kSlotsPerHinge + K; }
 struct EnvState {
   float pos[3], quat[4], q[kNJ];
   float vw[3], wb[3], qd[kNJ];
-  float anchor[2 * kNC];
+};
+// One env's arrays that stay in memory during a step (SoA, element i of the
+// env at p[i * stride]): PD targets read once per hinge, contact anchors read
+// and written by the contacts, last-substep outputs (nullable).
+struct EnvIO {
+  const float* ctrl;
+  float* anchor;
+  float* foot_pos;
+  float* foot_vel;
+  float* cf;
+  size_t stride;
 };
 struct EnvParams {
   float mu, dmass, kp_scale, kd_scale;
-};
-struct StepOut {  // last-substep outputs (reference src/g1_kernel.cu:128-150)
-  float foot_pos[6], foot_vel[6], fn[kNC];
 };
 
 // Running FK values of one body: body-frame twist, gravity, world pose (legs only).
@@ -418,18 +443,22 @@ G1_HD void fk_body(FKNode& n, const EnvState& st, Scr& scr) {
     if constexpr (tree_ident(I)) {
       RT = n.R;
     } else {
+#pragma unroll
       for (int a = 0; a < 3; ++a)
+#pragma unroll
         for (int b = 0; b < 3; ++b)
           RT.m[3 * a + b] = n.R.m[3 * a + 0] * tree_rot(I, 0, b) + n.R.m[3 * a + 1] * tree_rot(I, 1, b) +
                             n.R.m[3 * a + 2] * tree_rot(I, 2, b);
     }
     M3 R = RT;  // columns i1, i2 mixed: R = RT A
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
       R.m[3 * a + i1] = c * RT.m[3 * a + i1] + s * RT.m[3 * a + i2];
       R.m[3 * a + i2] = c * RT.m[3 * a + i2] - s * RT.m[3 * a + i1];
     }
     constexpr float p0 = tree_pos(I, 0), p1 = tree_pos(I, 1), p2 = tree_pos(I, 2);
     V3 pw = mk3(0.f, 0.f, 0.f);
+#pragma unroll
     for (int a = 0; a < 3; ++a) pw.v[a] = n.R.m[3 * a + 0] * p0 + n.R.m[3 * a + 1] * p1 + n.R.m[3 * a + 2] * p2;
     n.P = add(n.P, pw);
     n.R = R;
@@ -457,7 +486,9 @@ template <int I, class Scr>
 G1_HD SV load_bias(Scr& scr) {
   SV r;
   if constexpr (I == 0) {
+#pragma unroll
     for (int k = 0; k < 3; ++k) r.a.v[k] = scr.get(kSlotPelvis + k);
+#pragma unroll
     for (int k = 0; k < 3; ++k) r.l.v[k] = scr.get(kSlotPelvis + 3 + k);
   } else {
     r.a = mk3(scr.template get<slot<I, 6>()>(), scr.template get<slot<I, 7>()>(), scr.template get<slot<I, 8>()>());
@@ -479,9 +510,11 @@ G1_HD void fk_chain(FKNode& n, const EnvState& st, Scr& scr) {
 // Eight spheres, four on each foot (reference src/g1_core.h:123-153).  The
 // world wrench about the foot origin is accumulated and rotated to the body
 // frame once.
-template <int K0, class Scr>
-G1_HD void foot_contacts(const FKNode& n, float* anchor, const StepConfig& cfg, float mu,
-                         float* fn_out, Scr& scr, SV& pA_foot) {
+template <int K0>
+G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const StepConfig& cfg, float mu,
+                         SV& pA_foot) {
+  float* anchor = io.anchor;
+  const size_t sd = io.stride;
   const V3 ww = mv(n.R, n.w);  // world angular velocity
   const V3 vo = mv(n.R, n.v);  // world velocity of the foot origin
   V3 F = mk3(0.f, 0.f, 0.f), Tq = mk3(0.f, 0.f, 0.f);
@@ -497,7 +530,7 @@ G1_HD void foot_contacts(const FKNode& n, float* anchor, const StepConfig& cfg, 
     const V3 vp = add(vo, crs(ww, rw));
     float fn = cfg.contact_kn * depth - cfg.contact_dn * vp.v[2];
     fn = fminf(fmaxf(fn, 0.0f), 500.0f);
-    float ax = anchor[2 * k], ay = anchor[2 * k + 1];
+    float ax = anchor[(2 * k) * sd], ay = anchor[(2 * k + 1) * sd];
     const bool fresh = ax >= kAnchorFree;
     ax = fresh ? px : ax;
     ay = fresh ? py : ay;
@@ -512,17 +545,17 @@ G1_HD void foot_contacts(const FKNode& n, float* anchor, const StepConfig& cfg, 
       ay = py + fty * inv_kt;
     }
     if (in) {
-      anchor[2 * k] = ax;
-      anchor[2 * k + 1] = ay;
+      anchor[(2 * k) * sd] = ax;
+      anchor[(2 * k + 1) * sd] = ay;
       const V3 f = mk3(ftx, fty, fn);
       F = add(F, f);
       Tq = add(Tq, crs(rw, f));
     } else {
       fn = 0.0f;
-      anchor[2 * k] = kAnchorFree;
-      anchor[2 * k + 1] = kAnchorFree;
+      anchor[(2 * k) * sd] = kAnchorFree;
+      anchor[(2 * k + 1) * sd] = kAnchorFree;
     }
-    fn_out[k] = fn;
+    if (last && io.cf) io.cf[k * sd] = fn;
   }
   pA_foot.a = sub(pA_foot.a, mtv(n.R, Tq));
   pA_foot.l = sub(pA_foot.l, mtv(n.R, F));
@@ -541,29 +574,41 @@ G1_HD void ai_to_parent_add(AI& acc, const AI& Ia, float c, float s) {
   S3 M = rotT_sym<I>(rotA_sym<AX>(Ia.M, c, s));
   if constexpr (!p_zero<I>()) {
     float Mf[9];
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = 0; b < 3; ++b) Mf[3 * a + b] = M.s[sidx(a, b)];
     // H' = H + P M : (P M)[r][col] = (p x M[:,col])_r
     M3 Hn = H;
+#pragma unroll
     for (int col = 0; col < 3; ++col) {
       V3 mc = mk3(Mf[col], Mf[3 + col], Mf[6 + col]);
       V3 pm = pcross<I>(mc);
+#pragma unroll
       for (int r = 0; r < 3; ++r) Hn.m[3 * r + col] = H.m[3 * r + col] + pm.v[r];
     }
     // J' = J + P H^T - H' P ; (P H^T)[r][c] = (p x H[c,:]^T)_r ; (H' P)[r][c] = -(p x H'[r,:]^T)_c
     V3 pHT[3], HnP[3];
+#pragma unroll
     for (int cc = 0; cc < 3; ++cc) pHT[cc] = pcross<I>(mk3(H.m[3 * cc], H.m[3 * cc + 1], H.m[3 * cc + 2]));
+#pragma unroll
     for (int r = 0; r < 3; ++r) HnP[r] = pcross<I>(mk3(Hn.m[3 * r], Hn.m[3 * r + 1], Hn.m[3 * r + 2]));
+#pragma unroll
     for (int r = 0; r < 3; ++r)
+#pragma unroll
       for (int cc = r; cc < 3; ++cc) {
         // (P H^T)[r][cc] = pHT[cc].v[r] ; (H' P)[r][cc] = -HnP[r].v[cc]
         acc.J.s[sidx(r, cc)] += J.s[sidx(r, cc)] + pHT[cc].v[r] + HnP[r].v[cc];
       }
+#pragma unroll
     for (int k = 0; k < 9; ++k) acc.H.m[k] += Hn.m[k];
   } else {
+#pragma unroll
     for (int k = 0; k < 6; ++k) acc.J.s[k] += J.s[k];
+#pragma unroll
     for (int k = 0; k < 9; ++k) acc.H.m[k] += H.m[k];
   }
+#pragma unroll
   for (int k = 0; k < 6; ++k) acc.M.s[k] += M.s[k];
 }
 
@@ -583,13 +628,15 @@ G1_HD SV f_to_parent(const SV& f, float c, float s) {
 // articulated inertia and bias; adds the projected values into (accI, accP).
 template <int I, class Scr>
 G1_HD void bwd_body(const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvState& st,
-                    const float* ctrl, const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
+                    const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
   constexpr int h = I - 1, AX = axis_of(I);
   constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
   const float c = scr.template get<slot<I, 0>()>(), s = scr.template get<slot<I, 1>()>();
   // U = IA S: column AX of J, row AX of H
   SV U;
+#pragma unroll
   for (int a = 0; a < 3; ++a) U.a.v[a] = IA.J.s[sidx(a, AX)];
+#pragma unroll
   for (int a = 0; a < 3; ++a) U.l.v[a] = IA.H.m[3 * AX + a];
   const float q = st.q[h], qd = st.qd[h];
   constexpr float kp0 = f_of(g1m_act_kp[h]), kv0 = f_of(g1m_act_kv[h]);
@@ -597,7 +644,7 @@ G1_HD void bwd_body(const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvSta
   constexpr float lo = f_of(g1m_jnt_range[2 * h]), hi = f_of(g1m_jnt_range[2 * h + 1]);
   constexpr float arm = f_of(g1m_armature[h]), damp = f_of(g1m_damping[h]);
   const float kp = kp0 * ep.kp_scale, kv = kv0 * ep.kd_scale;
-  float t = kp * (ctrl[h] - q) - kv * qd;
+  float t = kp * (io.ctrl[h * io.stride] - q) - kv * qd;
   t = fminf(fmaxf(t, -lim), lim);
   float b = kv + damp;
   if (q < lo) {
@@ -625,16 +672,21 @@ G1_HD void bwd_body(const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvSta
   W.a = scl(invD, U.a);
   W.l = scl(invD, U.l);
   AI Ia;
+#pragma unroll
   for (int a = 0; a < 3; ++a)
+#pragma unroll
     for (int bb = a; bb < 3; ++bb) {
       Ia.J.s[sidx(a, bb)] = IA.J.s[sidx(a, bb)] - U.a.v[a] * W.a.v[bb];
       Ia.M.s[sidx(a, bb)] = IA.M.s[sidx(a, bb)] - U.l.v[a] * W.l.v[bb];
     }
+#pragma unroll
   for (int a = 0; a < 3; ++a)
+#pragma unroll
     for (int bb = 0; bb < 3; ++bb) Ia.H.m[3 * a + bb] = IA.H.m[3 * a + bb] - U.a.v[a] * W.l.v[bb];
   // pa = pA + Ia c + (u / D) U   (c has zero AX components)
   SV pa;
   const float uD = u * invD;
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
     pa.a.v[a] = pA.a.v[a] + Ia.J.s[sidx(a, i1)] * cv.a.v[i1] + Ia.J.s[sidx(a, i2)] * cv.a.v[i2] +
                 Ia.H.m[3 * a + i1] * cv.l.v[i1] + Ia.H.m[3 * a + i2] * cv.l.v[i2] + uD * U.a.v[a];
@@ -659,24 +711,24 @@ G1_HD void bwd_body(const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvSta
 // Backward pass over the serial chain FIRST..LAST (LAST -> FIRST); the
 // chain's first body adds into (accI, accP) of its parent.
 template <int FIRST, int I, class Scr>
-G1_HD void bwd_chain(AI& IA, SV& pA, AI& accI, SV& accP, const EnvState& st, const float* ctrl,
+G1_HD void bwd_chain(AI& IA, SV& pA, AI& accI, SV& accP, const EnvState& st, const EnvIO& io,
                      const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
   if constexpr (I == FIRST) {
-    bwd_body<I>(IA, pA, accI, accP, st, ctrl, ep, cfg, scr);
+    bwd_body<I>(IA, pA, accI, accP, st, io, ep, cfg, scr);
   } else {
     AI IAp = body_inertia<I - 1>();
     SV pAp = load_bias<I - 1>(scr);
-    bwd_body<I>(IA, pA, IAp, pAp, st, ctrl, ep, cfg, scr);
-    bwd_chain<FIRST, I - 1>(IAp, pAp, accI, accP, st, ctrl, ep, cfg, scr);
+    bwd_body<I>(IA, pA, IAp, pAp, st, io, ep, cfg, scr);
+    bwd_chain<FIRST, I - 1>(IAp, pAp, accI, accP, st, io, ep, cfg, scr);
   }
 }
 
 template <int FIRST, int LAST, class Scr>
-G1_HD void bwd_chain_from_leaf(AI& accI, SV& accP, const EnvState& st, const float* ctrl,
+G1_HD void bwd_chain_from_leaf(AI& accI, SV& accP, const EnvState& st, const EnvIO& io,
                                const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
   AI IA = body_inertia<LAST>();
   SV pA = load_bias<LAST>(scr);
-  bwd_chain<FIRST, LAST>(IA, pA, accI, accP, st, ctrl, ep, cfg, scr);
+  bwd_chain<FIRST, LAST>(IA, pA, accI, accP, st, io, ep, cfg, scr);
 }
 
 // ---------------------------------------------------------- base solve
@@ -684,7 +736,9 @@ G1_HD void bwd_chain_from_leaf(AI& accI, SV& accP, const EnvState& st, const flo
 // uses a packed Cholesky, src/spatial.h:254-278; same system).
 G1_HD SV base_solve(const AI& A, const SV& pA) {
   float m[6][6];
+#pragma unroll
   for (int a = 0; a < 3; ++a)
+#pragma unroll
     for (int b = 0; b < 3; ++b) {
       m[a][b] = A.J.s[sidx(a, b)];
       m[3 + a][3 + b] = A.M.s[sidx(a, b)];
@@ -771,83 +825,115 @@ G1_HD void quat_to_rot(const float* q, M3& R) {
 G1_HD void quat_normalized(const float* q, float* r) {
   const float n = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
   const float inv = 1.0f / n;
+#pragma unroll
   for (int k = 0; k < 4; ++k) r[k] = q[k] * inv;
 }
 
 // ----------------------------------------------------------------- step
-// One substep: FK -> contacts -> PD + ABA -> integrate (reference
-// src/g1_core.h:225-232).  out receives the foot kinematics of this
-// substep's FK (before integration) and the contact normal forces.
-template <class Scr>
-G1_HD void step(EnvState& st, const float* ctrl, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
-                StepOut& out) {
-  // ---- base
+// Base frame quantities from the state: rotation, body twist, body gravity.
+G1_HD void base_node(const EnvState& st, const StepConfig& cfg, FKNode& base) {
   float qn[4];
   quat_normalized(st.quat, qn);
-  FKNode base;
   quat_to_rot(qn, base.R);
   base.P = mk3(st.pos[0], st.pos[1], st.pos[2]);
   base.w = mk3(st.wb[0], st.wb[1], st.wb[2]);
   base.v = mtv(base.R, mk3(st.vw[0], st.vw[1], st.vw[2]));
   base.g = mk3(base.R.m[6] * cfg.gravity_z, base.R.m[7] * cfg.gravity_z, base.R.m[8] * cfg.gravity_z);
-  const AI I0 = pelvis_inertia(ep.dmass);
-  {
-    SV pA0 = bias_force<0>(I0, base.w, base.v, base.g);
-    for (int k = 0; k < 3; ++k) scr.put(kSlotPelvis + k, pA0.a.v[k]);
-    for (int k = 0; k < 3; ++k) scr.put(kSlotPelvis + 3 + k, pA0.l.v[k]);
-  }
-  // ---- FK + contacts, chain by chain
-  {
-    FKNode n = base;
-    fk_chain<1, 6, true>(n, st, scr);
-    SV pA6 = load_bias<6>(scr);
-    foot_contacts<0>(n, st.anchor, cfg, ep.mu, out.fn, scr, pA6);
-    store_bias<6>(pA6, scr);
-    for (int k = 0; k < 3; ++k) out.foot_pos[k] = n.P.v[k];
+}
+
+template <int FOOT_BODY, int K0>
+G1_HD void foot_outputs(const FKNode& n, const EnvIO& io, bool last) {
+  if (!last) return;
+  constexpr int o = K0 == 0 ? 0 : 3;
+  if (io.foot_pos)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) io.foot_pos[(o + k) * io.stride] = n.P.v[k];
+  if (io.foot_vel) {
     const V3 fv = mv(n.R, n.v);
-    for (int k = 0; k < 3; ++k) out.foot_vel[k] = fv.v[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) io.foot_vel[(o + k) * io.stride] = fv.v[k];
   }
+}
+
+// One substep: FK -> contacts -> PD + ABA -> integrate (reference
+// src/g1_core.h:225-232).  With last set, the foot kinematics of this
+// substep's FK (before integration) and the contact normal forces are
+// written to io's outputs.
+template <class Scr>
+G1_HD void step(EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
+                bool last) {
+  // ---- FK + bias forces + contacts, chain by chain
   {
-    FKNode n = base;
-    fk_chain<7, 12, true>(n, st, scr);
-    SV pA12 = load_bias<12>(scr);
-    foot_contacts<4>(n, st.anchor, cfg, ep.mu, out.fn, scr, pA12);
-    store_bias<12>(pA12, scr);
-    for (int k = 0; k < 3; ++k) out.foot_pos[3 + k] = n.P.v[k];
-    const V3 fv = mv(n.R, n.v);
-    for (int k = 0; k < 3; ++k) out.foot_vel[3 + k] = fv.v[k];
-  }
-  FKNode torso = base;
-  fk_chain<13, 15, false>(torso, st, scr);
-  {
-    FKNode n = torso;
-    fk_chain<16, 22, false>(n, st, scr);
-  }
-  {
-    FKNode n = torso;
-    fk_chain<23, 29, false>(n, st, scr);
+    FKNode base;
+    base_node(st, cfg, base);
+    {
+      const SV pA0 = bias_force<0>(pelvis_inertia(ep.dmass), base.w, base.v, base.g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) scr.put(kSlotPelvis + k, pA0.a.v[k]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) scr.put(kSlotPelvis + 3 + k, pA0.l.v[k]);
+    }
+    {
+      FKNode n = base;
+      fk_chain<1, 6, true>(n, st, scr);
+      SV pA6 = load_bias<6>(scr);
+      foot_contacts<0>(n, io, last, cfg, ep.mu, pA6);
+      store_bias<6>(pA6, scr);
+      foot_outputs<6, 0>(n, io, last);
+    }
+    {
+      FKNode n = base;
+      fk_chain<7, 12, true>(n, st, scr);
+      SV pA12 = load_bias<12>(scr);
+      foot_contacts<4>(n, io, last, cfg, ep.mu, pA12);
+      store_bias<12>(pA12, scr);
+      foot_outputs<12, 4>(n, io, last);
+    }
+    FKNode torso = base;
+    fk_chain<13, 15, false>(torso, st, scr);
+    {
+      FKNode n = torso;
+      fk_chain<16, 22, false>(n, st, scr);
+    }
+    {
+      FKNode n = torso;
+      fk_chain<23, 29, false>(n, st, scr);
+    }
   }
   // ---- backward: arms into the torso, waist into the pelvis, then legs
-  AI acc15 = body_inertia<15>();
-  SV accP15 = load_bias<15>(scr);
-  bwd_chain_from_leaf<16, 22>(acc15, accP15, st, ctrl, ep, cfg, scr);
-  bwd_chain_from_leaf<23, 29>(acc15, accP15, st, ctrl, ep, cfg, scr);
-  AI acc0 = I0;
-  SV accP0 = load_bias<0>(scr);
+  AI acc0;
+  SV accP0;
   {
+    AI acc15 = body_inertia<15>();
+    SV accP15 = load_bias<15>(scr);
+    bwd_chain_from_leaf<16, 22>(acc15, accP15, st, io, ep, cfg, scr);
+    bwd_chain_from_leaf<23, 29>(acc15, accP15, st, io, ep, cfg, scr);
+    acc0 = pelvis_inertia(ep.dmass);
+    accP0 = load_bias<0>(scr);
     AI IA14 = body_inertia<14>();
     SV pA14 = load_bias<14>(scr);
-    bwd_body<15>(acc15, accP15, IA14, pA14, st, ctrl, ep, cfg, scr);
+    bwd_body<15>(acc15, accP15, IA14, pA14, st, io, ep, cfg, scr);
     AI IA13 = body_inertia<13>();
     SV pA13 = load_bias<13>(scr);
-    bwd_body<14>(IA14, pA14, IA13, pA13, st, ctrl, ep, cfg, scr);
-    bwd_body<13>(IA13, pA13, acc0, accP0, st, ctrl, ep, cfg, scr);
+    bwd_body<14>(IA14, pA14, IA13, pA13, st, io, ep, cfg, scr);
+    bwd_body<13>(IA13, pA13, acc0, accP0, st, io, ep, cfg, scr);
   }
-  bwd_chain_from_leaf<1, 6>(acc0, accP0, st, ctrl, ep, cfg, scr);
-  bwd_chain_from_leaf<7, 12>(acc0, accP0, st, ctrl, ep, cfg, scr);
+  bwd_chain_from_leaf<1, 6>(acc0, accP0, st, io, ep, cfg, scr);
+  bwd_chain_from_leaf<7, 12>(acc0, accP0, st, io, ep, cfg, scr);
   // ---- base acceleration and forward pass (fused with integration)
   const SV a0 = base_solve(acc0, accP0);
   const float dt = cfg.dt;
+  // base: MuJoCo free-joint qacc (world linear incl. w x v, body angular);
+  // uses the pre-integration base frame, rebuilt from the unchanged state
+  {
+    FKNode base;
+    base_node(st, cfg, base);
+    const V3 al = mv(base.R, add(a0.l, crs(base.w, base.v)));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) st.vw[k] += dt * al.v[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
+  }
   fwd_chain<1, 6>(a0, st, dt, scr);
   fwd_chain<7, 12>(a0, st, dt, scr);
   {
@@ -858,11 +944,9 @@ G1_HD void step(EnvState& st, const float* ctrl, const EnvParams& ep, const Step
     fwd_chain<16, 22>(a, st, dt, scr);
     fwd_chain<23, 29>(a, st, dt, scr);
   }
-  // ---- base: MuJoCo free-joint qacc (world linear, body angular) + Euler
+  // ---- base position and orientation (semi-implicit Euler)
   {
-    const V3 al = mv(base.R, add(a0.l, crs(base.w, base.v)));
-    for (int k = 0; k < 3; ++k) st.vw[k] += dt * al.v[k];
-    for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
+#pragma unroll
     for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
     // q <- q (x) exp(w dt / 2), renormalised (reference src/spatial.h:73-79)
     const float wx = st.wb[0], wy = st.wb[1], wz = st.wb[2];
