@@ -26,12 +26,12 @@
 namespace g1b {
 
 // ------------------------------------------------------------ scratch
-// volatile: the compiler must not forward a stored value to its later load
-// (same thread, same address), which would turn the whole scratch back into
-// long-lived registers and spill them.
+// Slot-major per-thread scratch: p[slot * BLOCK].  Every phase of the step
+// writes and reads it at run-time slot indices from separate loops, so the
+// values are not forwarded into long-lived registers.
 template <int BLOCK>
 struct SmemScratch {
-  volatile float* p;
+  float* p;
   template <int K>
   __host__ __device__ __forceinline__ float get() const { return p[K * BLOCK]; }
   template <int K>
@@ -57,36 +57,32 @@ struct StateArgs {
   const float* kd_scale;
 };
 
-__device__ __forceinline__ void load_state(const StateArgs& a, int e, EnvState& st) {
+template <class Scr>
+__device__ __forceinline__ void load_state(const StateArgs& a, int e, EnvState& st, Scr& scr) {
   const size_t n = (size_t)a.nenv;
 #pragma unroll
   for (int k = 0; k < 3; ++k) st.pos[k] = a.qpos[k * n + e];
 #pragma unroll
   for (int k = 0; k < 4; ++k) st.quat[k] = a.qpos[(3 + k) * n + e];
 #pragma unroll
-  for (int k = 0; k < kNJ; ++k) st.q[k] = a.qpos[(7 + k) * n + e];
-#pragma unroll
   for (int k = 0; k < 3; ++k) st.vw[k] = a.qvel[k * n + e];
 #pragma unroll
   for (int k = 0; k < 3; ++k) st.wb[k] = a.qvel[(3 + k) * n + e];
-#pragma unroll
-  for (int k = 0; k < kNJ; ++k) st.qd[k] = a.qvel[(6 + k) * n + e];
+  load_joints(a.qpos + e, a.qvel + e, n, scr);
 }
 
-__device__ __forceinline__ void store_state(const StateArgs& a, int e, const EnvState& st) {
+template <class Scr>
+__device__ __forceinline__ void store_state(const StateArgs& a, int e, const EnvState& st, Scr& scr) {
   const size_t n = (size_t)a.nenv;
 #pragma unroll
   for (int k = 0; k < 3; ++k) a.qpos[k * n + e] = st.pos[k];
 #pragma unroll
   for (int k = 0; k < 4; ++k) a.qpos[(3 + k) * n + e] = st.quat[k];
 #pragma unroll
-  for (int k = 0; k < kNJ; ++k) a.qpos[(7 + k) * n + e] = st.q[k];
-#pragma unroll
   for (int k = 0; k < 3; ++k) a.qvel[k * n + e] = st.vw[k];
 #pragma unroll
   for (int k = 0; k < 3; ++k) a.qvel[(3 + k) * n + e] = st.wb[k];
-#pragma unroll
-  for (int k = 0; k < kNJ; ++k) a.qvel[(6 + k) * n + e] = st.qd[k];
+  store_joints(a.qpos + e, a.qvel + e, n, scr);
 }
 
 // The env's in-memory arrays (ctrl, anchors, outputs), offset to env e.
@@ -120,11 +116,11 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(StateArgs a, const float* _
   const int n = a.nenv;
   for (int e = blockIdx.x * BLOCK + threadIdx.x; e < n; e += gridDim.x * BLOCK) {
     EnvState st;
-    load_state(a, e, st);
+    load_state(a, e, st, scr);
     const EnvIO io = env_io(a, ctrl, e);
     const EnvParams ep = load_params(a, e);
     for (int s = 0; s < nsub; ++s) step(st, io, ep, cfg, scr, s == nsub - 1);
-    store_state(a, e, st);
+    store_state(a, e, st, scr);
   }
 }
 
@@ -180,7 +176,7 @@ __global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* ctrl
   const int n = a.nenv;
   for (int e = blockIdx.x * BLOCK + threadIdx.x; e < n; e += gridDim.x * BLOCK) {
     EnvState st;
-    load_state(a, e, st);
+    load_state(a, e, st, scr);
     const EnvIO io = env_io(a, ctrl, e);
     const EnvParams ep = load_params(a, e);
     int resets = 0;
@@ -192,22 +188,23 @@ __global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* ctrl
         const float u = uniform24(rp.seed ^ 0x5bd1e995u, (unsigned)e, (unsigned)stp);
         const float z0 = __fadd_rn(rp.z0_lo, __fmul_rn(u, __fsub_rn(rp.z0_hi, rp.z0_lo)));
 #pragma unroll
-        for (int i = 0; i < 3; ++i) st.pos[i] = stand_at(i);
+        for (int i = 0; i < 3; ++i) st.pos[i] = model().stand[i];
         st.pos[2] = z0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) st.quat[i] = stand_at(3 + i);
-#pragma unroll
-        for (int i = 0; i < kNJ; ++i) st.q[i] = stand_at(7 + i);
+        for (int i = 0; i < 4; ++i) st.quat[i] = model().stand[3 + i];
+#pragma unroll 1
+        for (int i = 0; i < kNJ; ++i) {
+          scr.put(hslot(i + 1, 0), model().stand[7 + i]);
+          scr.put(hslot(i + 1, 1), 0.0f);
+        }
 #pragma unroll
         for (int i = 0; i < 3; ++i) st.vw[i] = st.wb[i] = 0.0f;
-#pragma unroll
-        for (int i = 0; i < kNJ; ++i) st.qd[i] = 0.0f;
 #pragma unroll
         for (int i = 0; i < 2 * kNC; ++i) a.anchor[(size_t)i * n + e] = kAnchorFree;
         ++resets;
       }
     }
-    store_state(a, e, st);
+    store_state(a, e, st, scr);
     if (reset_count) reset_count[e] += resets;
   }
 }
@@ -223,7 +220,7 @@ __global__ void reset_done_kernel(int nenv, float* qpos, float* qvel, float* anc
   unsigned s = hash32(seed ^ (unsigned)(e + 1));
 #pragma unroll
   for (int i = 0; i < kNQ; ++i) {
-    float v = stand_at(i);
+    float v = model().stand[i];
     if (i == 2) v = __fadd_rn(v, drop);
     if (i >= 7) {
       s = hash32(s + 0x9E3779B9u);

@@ -1,6 +1,6 @@
-// g1_phys.cuh -- FP32 G1 step specialised at compile time on the G1 tree.
+// g1_phys.cuh -- FP32 G1 step for one environment per thread.
 //
-// One environment per thread.  The step is the reference's
+// The step is the reference's
 //   FK + velocities          (reference src/g1_core.h:29-54)
 //   contacts, PD, ABA        (reference src/g1_core.h:109-207)
 //   semi-implicit Euler      (reference src/g1_core.h:212-222)
@@ -8,18 +8,25 @@
 //   * every hinge axis is +x, +y or +z and every joint anchor is the body
 //     origin, so S = [e_ax; 0]: U = IA S is a column of IA, S^T f picks one
 //     component, the joint rotation mixes two coordinates with (cos, sin);
-//   * tree rotations, tree offsets and rigid-body spatial inertias are
-//     compile-time constants (no per-step quat_to_mat / spatial_inertia);
+//     each per-hinge routine exists in three axis-specialised copies and is
+//     dispatched by a warp-uniform switch (all threads of a warp process the
+//     same hinge);
+//   * tree rotations, tree offsets, rigid-body spatial inertias and servo
+//     parameters are precomputed per body in a constant table (no per-step
+//     quat_to_mat / spatial_inertia);
 //   * the tree is 5 serial chains (left leg 1-6, right leg 7-12, waist 13-15,
 //     left arm 16-22, right arm 23-29) hanging off the pelvis (0) and the
-//     torso (15), so the backward pass keeps ONE running articulated inertia
-//     per chain plus accumulators at the two branch bodies;
+//     torso (15); each phase loops over a chain's hinges, so the backward
+//     pass keeps ONE running articulated inertia per chain plus accumulators
+//     at the two branch bodies, and the code stays small enough for the
+//     instruction cache;
 //   * articulated inertias are kept as blocks J (sym), H (3x3), M (sym),
-//     transformed child->parent by the axis rotation (2-plane mix), the
-//     constant tree rotation and the constant offset;
+//     moved child->parent by the axis rotation (2-plane mix), the tree
+//     rotation and the offset;
 //   * contacts run right after each foot's FK and add a world-frame wrench.
-// Per-hinge values that the forward pass needs (cos/sin, velocity-product
-// term c, U, u, 1/D) live in a Scratch (shared memory on the device).
+// Per-hinge values the later passes need (joint angle and rate, cos/sin,
+// velocity-product term c, bias force then U, u, 1/D) live in a Scratch
+// (shared memory on the device).
 //
 // The header compiles as host code too (G1_HD) so that the same arithmetic
 // can be examined on the CPU; the product only runs it on the device.
@@ -42,77 +49,74 @@ constexpr int kNB = G1M_NB, kNJ = G1M_NB - 1, kNQ = G1M_NQ, kNV = G1M_NV, kNU = 
 constexpr int kNC = G1M_NC;
 constexpr float kAnchorFree = 1e30f;
 
-// ------------------------------------------------------------ model access
-// constexpr accessors: ONLY for constant expressions (if constexpr, constexpr
-// locals).  In device code a constexpr function reading these host tables with
-// a run-time argument would read host memory; run-time reads go through the
-// float mirrors below (tree_rot, spi).
-// consteval: a run-time call is a compile error, on the host and the device.
-#if defined(__cpp_consteval)
-#define G1_CONSTEVAL consteval
-#else
-#define G1_CONSTEVAL constexpr
-#endif
-G1_CONSTEVAL int parent_of(int i) { return g1m_parent[i]; }
-G1_CONSTEVAL int axis_of(int i) { return g1m_axis_idx[i - 1]; }
-G1_CONSTEVAL bool tree_ident(int i) { return g1m_tree_ident[i] != 0; }
-G1_CONSTEVAL float tree_pos(int i, int k) { return (float)g1m_tree_pos[3 * i + k]; }
-G1_CONSTEVAL float spi_c(int i, int k) { return (float)g1m_sp_inertia[16 * i + k]; }
-G1_CE float f_of(double x) { return (float)x; }
-
-// Float copies of the tables that device code indexes at run time (the
-// constexpr double tables are only usable in constant expressions there).
-template <int N>
-struct FTab {
-  float v[N];
-};
-template <int N>
-constexpr FTab<N> ftab(const double* src) {
-  FTab<N> t{};
-#pragma unroll
-  for (int i = 0; i < N; ++i) t.v[i] = (float)src[i];
-  return t;
-}
-#if defined(__CUDACC__)
-static __constant__ FTab<G1M_NQ> c_stand = ftab<G1M_NQ>(g1m_qpos_stand);
-static __constant__ FTab<3 * G1M_NC> c_contact_pos = ftab<3 * G1M_NC>(g1m_contact_pos);
-static __constant__ FTab<9 * G1M_NB> c_tree_rot = ftab<9 * G1M_NB>(g1m_tree_rot);
-static __constant__ FTab<16 * G1M_NB> c_spi = ftab<16 * G1M_NB>(g1m_sp_inertia);
-#endif
-// run-time accessors (constant-bank loads on the device)
-G1_HD float tree_rot(int i, int r, int c) {
-#if defined(__CUDA_ARCH__)
-  return c_tree_rot.v[9 * i + 3 * r + c];
-#else
-  return (float)g1m_tree_rot[9 * i + 3 * r + c];
-#endif
-}
-G1_HD float spi(int i, int k) {
-#if defined(__CUDA_ARCH__)
-  return c_spi.v[16 * i + k];
-#else
-  return (float)g1m_sp_inertia[16 * i + k];
-#endif
-}
-G1_HD float stand_at(int i) {
-#if defined(__CUDA_ARCH__)
-  return c_stand.v[i];
-#else
-  return (float)g1m_qpos_stand[i];
-#endif
-}
-G1_HD float contact_pos_at(int i) {
-#if defined(__CUDA_ARCH__)
-  return c_contact_pos.v[i];
-#else
-  return (float)g1m_contact_pos[i];
-#endif
-}
-
 // Per-step configuration (mirrors the reference G1Config, src/g1_types.h:33-42).
 struct StepConfig {
   float gravity_z, contact_kn, contact_dn, contact_kt, contact_dt, limit_kp, limit_kd, dt;
 };
+
+// ------------------------------------------------------------ model table
+// Everything one body contributes, in float.  Built at compile time from the
+// generated double tables; on the device it lives in constant memory and is
+// indexed by a warp-uniform body index.
+struct BodyC {
+  float T[9];        // tree rotation (parent <- body, before the joint), row-major
+  float p[3];        // body origin in the parent frame
+  float J[6], H[9];  // rigid spatial inertia at the origin: J (xx yy zz xy xz yz), H = m [c]x
+  float m;
+  float kp, kv, lim, lo, hi, arm, damp;  // servo and joint (hinges only)
+  int axis, ident;
+};
+struct ModelC {
+  BodyC b[kNB];
+  float stand[kNQ];
+  float contact_pos[3 * kNC];
+  float com0[3], icom0[6];  // pelvis COM and rotational inertia about it
+};
+constexpr ModelC make_model() {
+  ModelC M{};
+  for (int i = 0; i < kNB; ++i) {
+    BodyC& b = M.b[i];
+    for (int k = 0; k < 9; ++k) b.T[k] = (float)g1m_tree_rot[9 * i + k];
+    for (int k = 0; k < 3; ++k) b.p[k] = (float)g1m_tree_pos[3 * i + k];
+    for (int k = 0; k < 6; ++k) b.J[k] = (float)g1m_sp_inertia[16 * i + k];
+    for (int k = 0; k < 9; ++k) b.H[k] = (float)g1m_sp_inertia[16 * i + 6 + k];
+    b.m = (float)g1m_sp_inertia[16 * i + 15];
+    b.ident = g1m_tree_ident[i];
+    if (i > 0) {
+      const int h = i - 1;
+      b.kp = (float)g1m_act_kp[h];
+      b.kv = (float)g1m_act_kv[h];
+      b.lim = (float)g1m_act_frclim[h];
+      b.lo = (float)g1m_jnt_range[2 * h];
+      b.hi = (float)g1m_jnt_range[2 * h + 1];
+      b.arm = (float)g1m_armature[h];
+      b.damp = (float)g1m_damping[h];
+      b.axis = g1m_axis_idx[h];
+    }
+  }
+  for (int k = 0; k < kNQ; ++k) M.stand[k] = (float)g1m_qpos_stand[k];
+  for (int k = 0; k < 3 * kNC; ++k) M.contact_pos[k] = (float)g1m_contact_pos[k];
+  for (int k = 0; k < 3; ++k) M.com0[k] = (float)g1m_com[k];
+  M.icom0[0] = (float)g1m_inertia_com[0];
+  M.icom0[1] = (float)g1m_inertia_com[4];
+  M.icom0[2] = (float)g1m_inertia_com[8];
+  M.icom0[3] = (float)g1m_inertia_com[1];
+  M.icom0[4] = (float)g1m_inertia_com[2];
+  M.icom0[5] = (float)g1m_inertia_com[5];
+  return M;
+}
+#if defined(__CUDACC__)
+static __constant__ ModelC c_model = make_model();
+#endif
+static constexpr ModelC kModel = make_model();
+G1_HD const ModelC& model() {
+#if defined(__CUDA_ARCH__)
+  return c_model;
+#else
+  return kModel;
+#endif
+}
+G1_HD const BodyC& body(int i) { return model().b[i]; }
 
 // ----------------------------------------------------------------- algebra
 struct V3 {
@@ -126,7 +130,6 @@ G1_HD V3 crs(const V3& a, const V3& b) {
   return mk3(a.v[1] * b.v[2] - a.v[2] * b.v[1], a.v[2] * b.v[0] - a.v[0] * b.v[2],
              a.v[0] * b.v[1] - a.v[1] * b.v[0]);
 }
-G1_HD float dot(const V3& a, const V3& b) { return a.v[0] * b.v[0] + a.v[1] * b.v[1] + a.v[2] * b.v[2]; }
 
 // 3x3 row-major
 struct M3 {
@@ -147,7 +150,6 @@ G1_HD V3 mtv(const M3& A, const V3& x) {
 struct S3 {
   float s[6];
 };
-// pure helper called with run-time indices: must be a device function too
 G1_CE int sidx(int r, int c) {
   return r == c ? r : ((r == 0 && c == 1) || (r == 1 && c == 0)) ? 3 : ((r == 0 && c == 2) || (r == 2 && c == 0)) ? 4 : 5;
 }
@@ -158,7 +160,6 @@ struct AI {
   M3 H;
   S3 M;
 };
-
 struct SV {
   V3 a, l;
 };
@@ -188,7 +189,6 @@ G1_HD S3 rotA_sym(const S3& S, float c, float s) {
   constexpr int k = AX, i = (AX + 1) % 3, j = (AX + 2) % 3;
   const float sii = S.s[sidx(i, i)], sjj = S.s[sidx(j, j)], sij = S.s[sidx(i, j)];
   const float sik = S.s[sidx(i, k)], sjk = S.s[sidx(j, k)];
-  // B = A S, rows i and j
   const float bii = c * sii - s * sij, bij = c * sij - s * sjj;
   const float bji = s * sii + c * sij, bjj = s * sij + c * sjj;
   S3 r;
@@ -204,13 +204,13 @@ G1_HD S3 rotA_sym(const S3& S, float c, float s) {
 template <int AX>
 G1_HD M3 rotA_gen(const M3& H, float c, float s) {
   constexpr int i = (AX + 1) % 3, j = (AX + 2) % 3;
-  M3 B = H;  // B = A H: rows
+  M3 B = H;
 #pragma unroll
   for (int col = 0; col < 3; ++col) {
     B.m[3 * i + col] = c * H.m[3 * i + col] - s * H.m[3 * j + col];
     B.m[3 * j + col] = s * H.m[3 * i + col] + c * H.m[3 * j + col];
   }
-  M3 r = B;  // r = B A^T: columns
+  M3 r = B;
 #pragma unroll
   for (int row = 0; row < 3; ++row) {
     r.m[3 * row + i] = c * B.m[3 * row + i] - s * B.m[3 * row + j];
@@ -219,110 +219,63 @@ G1_HD M3 rotA_gen(const M3& H, float c, float s) {
   return r;
 }
 
-// ------------------------------------------- constant tree rotation (T)
-template <int I>
-G1_HD V3 rotT(const V3& x) {
-  if constexpr (tree_ident(I)) {
-    return x;
-  } else {
-    V3 r;
+// ---------------------------------------- tree rotation T (from the table)
+G1_HD V3 rotT(const BodyC& b, const V3& x) {
+  if (b.ident) return x;
+  V3 r;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-      r.v[a] = tree_rot(I, a, 0) * x.v[0] + tree_rot(I, a, 1) * x.v[1] + tree_rot(I, a, 2) * x.v[2];
-    return r;
-  }
+  for (int a = 0; a < 3; ++a) r.v[a] = b.T[3 * a] * x.v[0] + b.T[3 * a + 1] * x.v[1] + b.T[3 * a + 2] * x.v[2];
+  return r;
 }
-template <int I>
-G1_HD V3 rotTT(const V3& x) {
-  if constexpr (tree_ident(I)) {
-    return x;
-  } else {
-    V3 r;
+G1_HD V3 rotTT(const BodyC& b, const V3& x) {
+  if (b.ident) return x;
+  V3 r;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-      r.v[a] = tree_rot(I, 0, a) * x.v[0] + tree_rot(I, 1, a) * x.v[1] + tree_rot(I, 2, a) * x.v[2];
-    return r;
-  }
+  for (int a = 0; a < 3; ++a) r.v[a] = b.T[a] * x.v[0] + b.T[3 + a] * x.v[1] + b.T[6 + a] * x.v[2];
+  return r;
 }
-template <int I>
-G1_HD S3 rotT_sym(const S3& S) {
-  if constexpr (tree_ident(I)) {
-    return S;
-  } else {
-    float F[9];
+G1_HD void rotT_sym(const BodyC& b, S3& S) {  // S <- T S T^T
+  float B[9];
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
-        F[3 * a + b] = S.s[sidx(a, b)];
-    float B[9];
+    for (int c = 0; c < 3; ++c)
+      B[3 * a + c] = b.T[3 * a] * S.s[sidx(0, c)] + b.T[3 * a + 1] * S.s[sidx(1, c)] + b.T[3 * a + 2] * S.s[sidx(2, c)];
+  S3 r;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
-        B[3 * a + b] = tree_rot(I, a, 0) * F[b] + tree_rot(I, a, 1) * F[3 + b] + tree_rot(I, a, 2) * F[6 + b];
-    S3 r;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = a; b < 3; ++b)
-        r.s[sidx(a, b)] = B[3 * a + 0] * tree_rot(I, b, 0) + B[3 * a + 1] * tree_rot(I, b, 1) +
-                          B[3 * a + 2] * tree_rot(I, b, 2);
-    return r;
-  }
+    for (int c = a; c < 3; ++c)
+      r.s[sidx(a, c)] = B[3 * a] * b.T[3 * c] + B[3 * a + 1] * b.T[3 * c + 1] + B[3 * a + 2] * b.T[3 * c + 2];
+  S = r;
 }
-template <int I>
-G1_HD M3 rotT_gen(const M3& H) {
-  if constexpr (tree_ident(I)) {
-    return H;
-  } else {
-    float B[9];
+G1_HD void rotT_gen(const BodyC& b, M3& H) {  // H <- T H T^T
+  float B[9];
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
-        B[3 * a + b] = tree_rot(I, a, 0) * H.m[b] + tree_rot(I, a, 1) * H.m[3 + b] + tree_rot(I, a, 2) * H.m[6 + b];
-    M3 r;
+    for (int c = 0; c < 3; ++c) B[3 * a + c] = b.T[3 * a] * H.m[c] + b.T[3 * a + 1] * H.m[3 + c] + b.T[3 * a + 2] * H.m[6 + c];
+  M3 r;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
-        r.m[3 * a + b] = B[3 * a + 0] * tree_rot(I, b, 0) + B[3 * a + 1] * tree_rot(I, b, 1) +
-                         B[3 * a + 2] * tree_rot(I, b, 2);
-    return r;
-  }
+    for (int c = 0; c < 3; ++c)
+      r.m[3 * a + c] = B[3 * a] * b.T[3 * c] + B[3 * a + 1] * b.T[3 * c + 1] + B[3 * a + 2] * b.T[3 * c + 2];
+  H = r;
 }
-
-// ----------------------------------------- constant offset p (tree_pos)
-// p x v, term by term so that the zero components of p drop out.
-template <int I, int R>
-G1_HD float pcross_c(const V3& x) {
-  constexpr int a = (R + 1) % 3, b = (R + 2) % 3;
-  constexpr float pa = tree_pos(I, a), pb = tree_pos(I, b);
-  if constexpr (pa != 0.0f && pb != 0.0f) return pa * x.v[b] - pb * x.v[a];
-  else if constexpr (pa != 0.0f) return pa * x.v[b];
-  else if constexpr (pb != 0.0f) return -(pb * x.v[a]);
-  else return 0.0f;
-}
-template <int I>
-G1_HD V3 pcross(const V3& x) {
-  return mk3(pcross_c<I, 0>(x), pcross_c<I, 1>(x), pcross_c<I, 2>(x));
-}
-template <int I>
-G1_CONSTEVAL bool p_zero() {
-  return tree_pos(I, 0) == 0.0f && tree_pos(I, 1) == 0.0f && tree_pos(I, 2) == 0.0f;
+// p x v
+G1_HD V3 pcross(const BodyC& b, const V3& x) {
+  return mk3(b.p[1] * x.v[2] - b.p[2] * x.v[1], b.p[2] * x.v[0] - b.p[0] * x.v[2], b.p[0] * x.v[1] - b.p[1] * x.v[0]);
 }
 
 // --------------------------------------------------- rigid-body inertias
-template <int I>
-G1_HD AI body_inertia() {
+G1_HD AI body_inertia(const BodyC& b) {
   AI r;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) r.J.s[k] = spi(I, k);
+  for (int k = 0; k < 6; ++k) r.J.s[k] = b.J[k];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) r.H.m[k] = spi(I, 6 + k);
-  const float m = spi(I, 15);
-  r.M.s[0] = r.M.s[1] = r.M.s[2] = m;
+  for (int k = 0; k < 9; ++k) r.H.m[k] = b.H[k];
+  r.M.s[0] = r.M.s[1] = r.M.s[2] = b.m;
   r.M.s[3] = r.M.s[4] = r.M.s[5] = 0.0f;
   return r;
 }
@@ -330,21 +283,16 @@ G1_HD AI body_inertia() {
 // Pelvis inertia with a per-env mass offset (COM and rotational inertia
 // about the COM unchanged): J = Icom + m [c]x [c]x^T, H = m [c]x, M = m 1.
 G1_HD AI pelvis_inertia(float dmass) {
-  constexpr float m0 = spi_c(0, 15);
-  constexpr float cx = (float)g1m_com[0], cy = (float)g1m_com[1], cz = (float)g1m_com[2];
-  const float m = m0 + dmass;
+  const ModelC& M = model();
+  const float cx = M.com0[0], cy = M.com0[1], cz = M.com0[2];
+  const float m = M.b[0].m + dmass;
   AI r;
-  // Icom part of J = J0 - m0 [c]x[c]x^T, done in double at compile time
-  constexpr float icxx = (float)(g1m_inertia_com[0]), icyy = (float)(g1m_inertia_com[4]);
-  constexpr float iczz = (float)(g1m_inertia_com[8]), icxy = (float)(g1m_inertia_com[1]);
-  constexpr float icxz = (float)(g1m_inertia_com[2]), icyz = (float)(g1m_inertia_com[5]);
-  // [c]x [c]x^T = (c.c) 1 - c c^T
-  r.J.s[0] = icxx + m * (cy * cy + cz * cz);
-  r.J.s[1] = icyy + m * (cx * cx + cz * cz);
-  r.J.s[2] = iczz + m * (cx * cx + cy * cy);
-  r.J.s[3] = icxy - m * (cx * cy);
-  r.J.s[4] = icxz - m * (cx * cz);
-  r.J.s[5] = icyz - m * (cy * cz);
+  r.J.s[0] = M.icom0[0] + m * (cy * cy + cz * cz);
+  r.J.s[1] = M.icom0[1] + m * (cx * cx + cz * cz);
+  r.J.s[2] = M.icom0[2] + m * (cx * cx + cy * cy);
+  r.J.s[3] = M.icom0[3] - m * (cx * cy);
+  r.J.s[4] = M.icom0[4] - m * (cx * cz);
+  r.J.s[5] = M.icom0[5] - m * (cy * cz);
   r.H.m[0] = 0.0f;     r.H.m[1] = -m * cz; r.H.m[2] = m * cy;
   r.H.m[3] = m * cz;   r.H.m[4] = 0.0f;    r.H.m[5] = -m * cx;
   r.H.m[6] = -m * cy;  r.H.m[7] = m * cx;  r.H.m[8] = 0.0f;
@@ -353,49 +301,41 @@ G1_HD AI pelvis_inertia(float dmass) {
   return r;
 }
 
-// I v for a spatial inertia
-G1_HD SV ai_mul(const AI& I, const SV& x) {
-  SV r;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    r.a.v[a] = I.J.s[sidx(a, 0)] * x.a.v[0] + I.J.s[sidx(a, 1)] * x.a.v[1] + I.J.s[sidx(a, 2)] * x.a.v[2] +
-               I.H.m[3 * a + 0] * x.l.v[0] + I.H.m[3 * a + 1] * x.l.v[1] + I.H.m[3 * a + 2] * x.l.v[2];
-    r.l.v[a] = I.H.m[a] * x.a.v[0] + I.H.m[3 + a] * x.a.v[1] + I.H.m[6 + a] * x.a.v[2] +
-               I.M.s[sidx(a, 0)] * x.l.v[0] + I.M.s[sidx(a, 1)] * x.l.v[1] + I.M.s[sidx(a, 2)] * x.l.v[2];
-  }
-  return r;
-}
-
 // Rigid-body bias force with gravity (reference src/g1_core.h:113-120):
 //   pA = v x* (I v) - [c x (m g_b); m g_b],  [c x (m g); m g] = [H g; m g].
-template <int I>
 G1_HD SV bias_force(const AI& In, const V3& w, const V3& v, const V3& g) {
-  SV x{w, v};
-  SV h = ai_mul(In, x);
-  const float m = In.M.s[0];
+  V3 ha, hl;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    ha.v[a] = In.J.s[sidx(a, 0)] * w.v[0] + In.J.s[sidx(a, 1)] * w.v[1] + In.J.s[sidx(a, 2)] * w.v[2] +
+              In.H.m[3 * a] * v.v[0] + In.H.m[3 * a + 1] * v.v[1] + In.H.m[3 * a + 2] * v.v[2];
+    hl.v[a] = In.H.m[a] * w.v[0] + In.H.m[3 + a] * w.v[1] + In.H.m[6 + a] * w.v[2] + In.M.s[sidx(a, 0)] * v.v[0] +
+              In.M.s[sidx(a, 1)] * v.v[1] + In.M.s[sidx(a, 2)] * v.v[2];
+  }
+  const V3 hg = mk3(In.H.m[0] * g.v[0] + In.H.m[1] * g.v[1] + In.H.m[2] * g.v[2],
+                    In.H.m[3] * g.v[0] + In.H.m[4] * g.v[1] + In.H.m[5] * g.v[2],
+                    In.H.m[6] * g.v[0] + In.H.m[7] * g.v[1] + In.H.m[8] * g.v[2]);
   SV r;
-  V3 hg = mk3(In.H.m[0] * g.v[0] + In.H.m[1] * g.v[1] + In.H.m[2] * g.v[2],
-              In.H.m[3] * g.v[0] + In.H.m[4] * g.v[1] + In.H.m[5] * g.v[2],
-              In.H.m[6] * g.v[0] + In.H.m[7] * g.v[1] + In.H.m[8] * g.v[2]);
-  r.a = sub(add(crs(w, h.a), crs(v, h.l)), hg);
-  r.l = sub(crs(w, h.l), scl(m, g));
+  r.a = sub(add(crs(w, ha), crs(v, hl)), hg);
+  r.l = sub(crs(w, hl), scl(In.M.s[0], g));
   return r;
 }
 
 // ---------------------------------------------------------------- scratch
-// Per-hinge slots: 0-1 cos/sin, 2-5 velocity-product term c (4 non-zeros),
-// 6-11 bias force pA (FK -> backward) then U (backward -> forward),
-// 12 u, 13 1/D.  Slots 406-411: pelvis bias force.
-constexpr int kSlotsPerHinge = 14;
+// Per hinge h (body h + 1), slot h * 15 + k:
+//   0 q, 1 qd, 2 cos, 3 sin, 4-7 velocity-product term c (4 non-zeros),
+//   8-13 bias force pA (FK -> backward), then U / D (backward -> forward),
+//   14 u / D.
+// Slots kSlotPelvis.. +5: pelvis bias force.
+constexpr int kSlotsPerHinge = 15;
 constexpr int kSlotPelvis = kNJ * kSlotsPerHinge;
 constexpr int kNumSlots = kSlotPelvis + 6;
-template <int I, int K>
-G1_CONSTEVAL int slot() { return (I - 1) * kSlotsPerHinge + K; }
+G1_CE int hslot(int body, int k) { return (body - 1) * kSlotsPerHinge + k; }
 
 // ----------------------------------------------------------- env data
+// Base state kept in registers; joint angles and rates live in the scratch.
 struct EnvState {
-  float pos[3], quat[4], q[kNJ];
-  float vw[3], wb[3], qd[kNJ];
+  float pos[3], quat[4], vw[3], wb[3];
 };
 // One env's arrays that stay in memory during a step (SoA, element i of the
 // env at p[i * stride]): PD targets read once per hinge, contact anchors read
@@ -419,91 +359,86 @@ struct FKNode {
   V3 P;
 };
 
+template <class Scr>
+G1_HD void store_sv(Scr& scr, int s0, const SV& x) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) scr.put(s0 + k, x.a.v[k]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) scr.put(s0 + 3 + k, x.l.v[k]);
+}
+template <class Scr>
+G1_HD SV load_sv(Scr& scr, int s0) {
+  SV r;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) r.a.v[k] = scr.get(s0 + k);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) r.l.v[k] = scr.get(s0 + 3 + k);
+  return r;
+}
+template <class Scr>
+G1_HD SV load_bias(Scr& scr, int body) {
+  return load_sv(scr, body == 0 ? kSlotPelvis : hslot(body, 8));
+}
+
 // ------------------------------------------------------------- FK pass
-// reference src/g1_core.h:29-54 (+ bias init :113-120 and c of :180)
-template <int I, bool kWorld, class Scr>
-G1_HD void fk_body(FKNode& n, const EnvState& st, Scr& scr) {
-  constexpr int AX = axis_of(I);
+// reference src/g1_core.h:29-54 (+ bias init :113-120 and the c term of :180)
+template <int AX, bool kWorld, class Scr>
+G1_HD void fk_body(int i, FKNode& n, Scr& scr) {
   constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
-  const float q = st.q[I - 1], qd = st.qd[I - 1];
+  const BodyC& b = body(i);
+  const float q = scr.get(hslot(i, 0)), qd = scr.get(hslot(i, 1));
   float s, c;
   sincosf(q, &s, &c);
-  scr.template put<slot<I, 0>()>(c);
-  scr.template put<slot<I, 1>()>(s);
+  scr.put(hslot(i, 2), c);
+  scr.put(hslot(i, 3), s);
   // parent -> child: x_c = A^T T^T x_p ;  v.l uses v_p - p x w_p
-  V3 t = n.v;
-  if constexpr (!p_zero<I>()) t = sub(n.v, pcross<I>(n.w));
-  V3 w = rotAT<AX>(rotTT<I>(n.w), c, s);
-  V3 v = rotAT<AX>(rotTT<I>(t), c, s);
-  V3 g = rotAT<AX>(rotTT<I>(n.g), c, s);
+  const V3 t = sub(n.v, pcross(b, n.w));
+  V3 w = rotAT<AX>(rotTT(b, n.w), c, s);
+  const V3 v = rotAT<AX>(rotTT(b, t), c, s);
+  const V3 g = rotAT<AX>(rotTT(b, n.g), c, s);
   w.v[AX] += qd;
   if constexpr (kWorld) {
     // R_i = R_p T A ; P_i = P_p + R_p p
-    M3 RT;
-    if constexpr (tree_ident(I)) {
-      RT = n.R;
-    } else {
+    M3 RT = n.R;
+    if (!b.ident) {
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b)
-          RT.m[3 * a + b] = n.R.m[3 * a + 0] * tree_rot(I, 0, b) + n.R.m[3 * a + 1] * tree_rot(I, 1, b) +
-                            n.R.m[3 * a + 2] * tree_rot(I, 2, b);
+        for (int bb = 0; bb < 3; ++bb)
+          RT.m[3 * a + bb] = n.R.m[3 * a] * b.T[bb] + n.R.m[3 * a + 1] * b.T[3 + bb] + n.R.m[3 * a + 2] * b.T[6 + bb];
     }
-    M3 R = RT;  // columns i1, i2 mixed: R = RT A
+    M3 R = RT;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       R.m[3 * a + i1] = c * RT.m[3 * a + i1] + s * RT.m[3 * a + i2];
       R.m[3 * a + i2] = c * RT.m[3 * a + i2] - s * RT.m[3 * a + i1];
     }
-    constexpr float p0 = tree_pos(I, 0), p1 = tree_pos(I, 1), p2 = tree_pos(I, 2);
-    V3 pw = mk3(0.f, 0.f, 0.f);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) pw.v[a] = n.R.m[3 * a + 0] * p0 + n.R.m[3 * a + 1] * p1 + n.R.m[3 * a + 2] * p2;
-    n.P = add(n.P, pw);
+    n.P = add(n.P, mv(n.R, mk3(b.p[0], b.p[1], b.p[2])));
     n.R = R;
   }
   n.w = w;
   n.v = v;
   n.g = g;
   // velocity-product term c = v x_m (qd S) = [qd (w x e_ax); qd (v x e_ax)]
-  scr.template put<slot<I, 2>()>(qd * w.v[i2]);
-  scr.template put<slot<I, 3>()>(-(qd * w.v[i1]));
-  scr.template put<slot<I, 4>()>(qd * v.v[i2]);
-  scr.template put<slot<I, 5>()>(-(qd * v.v[i1]));
+  scr.put(hslot(i, 4), qd * w.v[i2]);
+  scr.put(hslot(i, 5), -(qd * w.v[i1]));
+  scr.put(hslot(i, 6), qd * v.v[i2]);
+  scr.put(hslot(i, 7), -(qd * v.v[i1]));
+  store_sv(scr, hslot(i, 8), bias_force(body_inertia(b), w, v, g));
 }
 
-template <int I, class Scr>
-G1_HD void store_bias(const SV& pA, Scr& scr) {
-  scr.template put<slot<I, 6>()>(pA.a.v[0]);
-  scr.template put<slot<I, 7>()>(pA.a.v[1]);
-  scr.template put<slot<I, 8>()>(pA.a.v[2]);
-  scr.template put<slot<I, 9>()>(pA.l.v[0]);
-  scr.template put<slot<I, 10>()>(pA.l.v[1]);
-  scr.template put<slot<I, 11>()>(pA.l.v[2]);
-}
-template <int I, class Scr>
-G1_HD SV load_bias(Scr& scr) {
-  SV r;
-  if constexpr (I == 0) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r.a.v[k] = scr.get(kSlotPelvis + k);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r.l.v[k] = scr.get(kSlotPelvis + 3 + k);
-  } else {
-    r.a = mk3(scr.template get<slot<I, 6>()>(), scr.template get<slot<I, 7>()>(), scr.template get<slot<I, 8>()>());
-    r.l = mk3(scr.template get<slot<I, 9>()>(), scr.template get<slot<I, 10>()>(), scr.template get<slot<I, 11>()>());
+// FK of the serial chain first..last from the node of its parent; stores
+// each body's bias force.
+template <bool kWorld, class Scr>
+G1_HD void fk_chain(int first, int last, FKNode& n, Scr& scr) {
+#pragma unroll 1
+  for (int i = first; i <= last; ++i) {
+    switch (body(i).axis) {
+      case 0: fk_body<0, kWorld>(i, n, scr); break;
+      case 1: fk_body<1, kWorld>(i, n, scr); break;
+      default: fk_body<2, kWorld>(i, n, scr); break;
+    }
   }
-  return r;
-}
-
-// FK of a serial chain FIRST..LAST (each body's parent is the previous one,
-// the first body's parent is the node passed in); stores biases.
-template <int I, int LAST, bool kWorld, class Scr>
-G1_HD void fk_chain(FKNode& n, const EnvState& st, Scr& scr) {
-  fk_body<I, kWorld>(n, st, scr);
-  if constexpr (I != 0) store_bias<I>(bias_force<I>(body_inertia<I>(), n.w, n.v, n.g), scr);
-  if constexpr (I < LAST) fk_chain<I + 1, LAST, kWorld>(n, st, scr);
 }
 
 // --------------------------------------------------------------- contacts
@@ -518,11 +453,12 @@ G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const Step
   const V3 ww = mv(n.R, n.w);  // world angular velocity
   const V3 vo = mv(n.R, n.v);  // world velocity of the foot origin
   V3 F = mk3(0.f, 0.f, 0.f), Tq = mk3(0.f, 0.f, 0.f);
-  constexpr float radius = (float)g1m_contact_radius;
+  const float radius = (float)g1m_contact_radius;
   const float inv_kt = 1.0f / cfg.contact_kt;
+  const ModelC& M = model();
 #pragma unroll
   for (int k = K0; k < K0 + 4; ++k) {
-    const V3 r = mk3(contact_pos_at(3 * k), contact_pos_at(3 * k + 1), contact_pos_at(3 * k + 2));
+    const V3 r = mk3(M.contact_pos[3 * k], M.contact_pos[3 * k + 1], M.contact_pos[3 * k + 2]);
     const V3 rw = mv(n.R, r);
     const float px = n.P.v[0] + rw.v[0], py = n.P.v[1] + rw.v[1], pz = n.P.v[2] + rw.v[2];
     const float depth = radius - pz;
@@ -562,111 +498,93 @@ G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const Step
 }
 
 // --------------------------------------------------------- backward pass
-// Transform child articulated inertia Ia (child frame) into the parent frame
-// and add it: X* Ia X^-1 with X = (R = T A, p).  Blocks after rotation
-// (J2, H2, M2) and then the offset P = [p]x:
+// Transform the child articulated inertia Ia (child frame) into the parent
+// frame and add it: X* Ia X^-1 with X = (R = T A, p).  Blocks after the
+// rotation (J2, H2, M2), then the offset P = [p]x:
 //   H' = H2 + P M2 ;  J' = J2 + P H2^T - H' P ;  M' = M2.
-template <int I>
-G1_HD void ai_to_parent_add(AI& acc, const AI& Ia, float c, float s) {
-  constexpr int AX = axis_of(I);
-  S3 J = rotT_sym<I>(rotA_sym<AX>(Ia.J, c, s));
-  M3 H = rotT_gen<I>(rotA_gen<AX>(Ia.H, c, s));
-  S3 M = rotT_sym<I>(rotA_sym<AX>(Ia.M, c, s));
-  if constexpr (!p_zero<I>()) {
-    float Mf[9];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) Mf[3 * a + b] = M.s[sidx(a, b)];
-    // H' = H + P M : (P M)[r][col] = (p x M[:,col])_r
-    M3 Hn = H;
-#pragma unroll
-    for (int col = 0; col < 3; ++col) {
-      V3 mc = mk3(Mf[col], Mf[3 + col], Mf[6 + col]);
-      V3 pm = pcross<I>(mc);
-#pragma unroll
-      for (int r = 0; r < 3; ++r) Hn.m[3 * r + col] = H.m[3 * r + col] + pm.v[r];
-    }
-    // J' = J + P H^T - H' P ; (P H^T)[r][c] = (p x H[c,:]^T)_r ; (H' P)[r][c] = -(p x H'[r,:]^T)_c
-    V3 pHT[3], HnP[3];
-#pragma unroll
-    for (int cc = 0; cc < 3; ++cc) pHT[cc] = pcross<I>(mk3(H.m[3 * cc], H.m[3 * cc + 1], H.m[3 * cc + 2]));
-#pragma unroll
-    for (int r = 0; r < 3; ++r) HnP[r] = pcross<I>(mk3(Hn.m[3 * r], Hn.m[3 * r + 1], Hn.m[3 * r + 2]));
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int cc = r; cc < 3; ++cc) {
-        // (P H^T)[r][cc] = pHT[cc].v[r] ; (H' P)[r][cc] = -HnP[r].v[cc]
-        acc.J.s[sidx(r, cc)] += J.s[sidx(r, cc)] + pHT[cc].v[r] + HnP[r].v[cc];
-      }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) acc.H.m[k] += Hn.m[k];
-  } else {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) acc.J.s[k] += J.s[k];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) acc.H.m[k] += H.m[k];
+template <int AX>
+G1_HD void ai_to_parent_add(const BodyC& b, AI& acc, const AI& Ia, float c, float s) {
+  S3 J = rotA_sym<AX>(Ia.J, c, s);
+  M3 H = rotA_gen<AX>(Ia.H, c, s);
+  S3 M = rotA_sym<AX>(Ia.M, c, s);
+  if (!b.ident) {
+    rotT_sym(b, J);
+    rotT_gen(b, H);
+    rotT_sym(b, M);
   }
+  // H' = H + P M : (P M)[r][col] = (p x M[:,col])_r
+  M3 Hn;
+#pragma unroll
+  for (int col = 0; col < 3; ++col) {
+    const V3 pm = pcross(b, mk3(M.s[sidx(0, col)], M.s[sidx(1, col)], M.s[sidx(2, col)]));
+#pragma unroll
+    for (int r = 0; r < 3; ++r) Hn.m[3 * r + col] = H.m[3 * r + col] + pm.v[r];
+  }
+  // J' = J + P H^T - H' P ; (P H^T)[r][c] = (p x H[c,:])_r ; (H' P)[r][c] = -(p x H'[r,:])_c
+  V3 pHT[3], HnP[3];
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) pHT[cc] = pcross(b, mk3(H.m[3 * cc], H.m[3 * cc + 1], H.m[3 * cc + 2]));
+#pragma unroll
+  for (int r = 0; r < 3; ++r) HnP[r] = pcross(b, mk3(Hn.m[3 * r], Hn.m[3 * r + 1], Hn.m[3 * r + 2]));
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int cc = r; cc < 3; ++cc) acc.J.s[sidx(r, cc)] += J.s[sidx(r, cc)] + pHT[cc].v[r] + HnP[r].v[cc];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) acc.H.m[k] += Hn.m[k];
 #pragma unroll
   for (int k = 0; k < 6; ++k) acc.M.s[k] += M.s[k];
 }
 
 // force child -> parent: [R f.a + p x (R f.l); R f.l]
-template <int I>
-G1_HD SV f_to_parent(const SV& f, float c, float s) {
-  constexpr int AX = axis_of(I);
+template <int AX>
+G1_HD SV f_to_parent(const BodyC& b, const SV& f, float c, float s) {
   SV r;
-  r.l = rotT<I>(rotA<AX>(f.l, c, s));
-  r.a = rotT<I>(rotA<AX>(f.a, c, s));
-  if constexpr (!p_zero<I>()) r.a = add(r.a, pcross<I>(r.l));
+  r.l = rotT(b, rotA<AX>(f.l, c, s));
+  r.a = add(rotT(b, rotA<AX>(f.a, c, s)), pcross(b, r.l));
   return r;
 }
 
 // One hinge of the backward pass with PD servo, soft limits and implicit
-// damping (reference src/g1_core.h:156-186).  IA, pA are body I's
-// articulated inertia and bias; adds the projected values into (accI, accP).
-template <int I, class Scr>
-G1_HD void bwd_body(const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvState& st,
-                    const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
-  constexpr int h = I - 1, AX = axis_of(I);
+// damping (reference src/g1_core.h:156-186).  IA, pA are body i's
+// articulated inertia and bias; the projected values are added into
+// (accI, accP), expressed in the parent's frame.
+template <int AX, class Scr>
+G1_HD void bwd_body(int i, const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvIO& io,
+                    const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
   constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
-  const float c = scr.template get<slot<I, 0>()>(), s = scr.template get<slot<I, 1>()>();
+  const BodyC& b = body(i);
+  const int h = i - 1;
+  const float c = scr.get(hslot(i, 2)), s = scr.get(hslot(i, 3));
   // U = IA S: column AX of J, row AX of H
   SV U;
 #pragma unroll
   for (int a = 0; a < 3; ++a) U.a.v[a] = IA.J.s[sidx(a, AX)];
 #pragma unroll
   for (int a = 0; a < 3; ++a) U.l.v[a] = IA.H.m[3 * AX + a];
-  const float q = st.q[h], qd = st.qd[h];
-  constexpr float kp0 = f_of(g1m_act_kp[h]), kv0 = f_of(g1m_act_kv[h]);
-  constexpr float lim = f_of(g1m_act_frclim[h]);
-  constexpr float lo = f_of(g1m_jnt_range[2 * h]), hi = f_of(g1m_jnt_range[2 * h + 1]);
-  constexpr float arm = f_of(g1m_armature[h]), damp = f_of(g1m_damping[h]);
-  const float kp = kp0 * ep.kp_scale, kv = kv0 * ep.kd_scale;
+  const float q = scr.get(hslot(i, 0)), qd = scr.get(hslot(i, 1));
+  const float kp = b.kp * ep.kp_scale, kv = b.kv * ep.kd_scale;
   float t = kp * (io.ctrl[h * io.stride] - q) - kv * qd;
-  t = fminf(fmaxf(t, -lim), lim);
-  float b = kv + damp;
-  if (q < lo) {
-    t += cfg.limit_kp * (lo - q) - cfg.limit_kd * qd;
-    b += cfg.limit_kd;
+  t = fminf(fmaxf(t, -b.lim), b.lim);
+  float bd = kv + b.damp;
+  if (q < b.lo) {
+    t += cfg.limit_kp * (b.lo - q) - cfg.limit_kd * qd;
+    bd += cfg.limit_kd;
   }
-  if (q > hi) {
-    t += cfg.limit_kp * (hi - q) - cfg.limit_kd * qd;
-    b += cfg.limit_kd;
+  if (q > b.hi) {
+    t += cfg.limit_kp * (b.hi - q) - cfg.limit_kd * qd;
+    bd += cfg.limit_kd;
   }
-  const float D = U.a.v[AX] + arm + cfg.dt * b;
-  float u = t - pA.a.v[AX];
-  if constexpr (damp != 0.0f) u -= damp * qd;
+  const float D = U.a.v[AX] + b.arm + cfg.dt * bd;
+  const float u = t - b.damp * qd - pA.a.v[AX];
   const float invD = 1.0f / D;
-  // c (velocity-product term): angular comps i1, i2 and linear comps i1, i2
   SV cv;
   cv.a.v[AX] = 0.0f;
-  cv.a.v[i1] = scr.template get<slot<I, 2>()>();
-  cv.a.v[i2] = scr.template get<slot<I, 3>()>();
+  cv.a.v[i1] = scr.get(hslot(i, 4));
+  cv.a.v[i2] = scr.get(hslot(i, 5));
   cv.l.v[AX] = 0.0f;
-  cv.l.v[i1] = scr.template get<slot<I, 4>()>();
-  cv.l.v[i2] = scr.template get<slot<I, 5>()>();
+  cv.l.v[i1] = scr.get(hslot(i, 6));
+  cv.l.v[i2] = scr.get(hslot(i, 7));
   // Ia = IA - U U^T / D
   SV W;
   W.a = scl(invD, U.a);
@@ -693,42 +611,59 @@ G1_HD void bwd_body(const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvSta
     pa.l.v[a] = pA.l.v[a] + Ia.H.m[3 * i1 + a] * cv.a.v[i1] + Ia.H.m[3 * i2 + a] * cv.a.v[i2] +
                 Ia.M.s[sidx(a, i1)] * cv.l.v[i1] + Ia.M.s[sidx(a, i2)] * cv.l.v[i2] + uD * U.l.v[a];
   }
-  // keep U, u, 1/D for the forward pass (in the bias slots)
-  scr.template put<slot<I, 6>()>(U.a.v[0]);
-  scr.template put<slot<I, 7>()>(U.a.v[1]);
-  scr.template put<slot<I, 8>()>(U.a.v[2]);
-  scr.template put<slot<I, 9>()>(U.l.v[0]);
-  scr.template put<slot<I, 10>()>(U.l.v[1]);
-  scr.template put<slot<I, 11>()>(U.l.v[2]);
-  scr.template put<slot<I, 12>()>(u);
-  scr.template put<slot<I, 13>()>(invD);
-  ai_to_parent_add<I>(accI, Ia, c, s);
-  const SV fp = f_to_parent<I>(pa, c, s);
+  // keep U / D and u / D for the forward pass (U / D in the bias slots)
+  store_sv(scr, hslot(i, 8), W);
+  scr.put(hslot(i, 14), uD);
+  ai_to_parent_add<AX>(b, accI, Ia, c, s);
+  const SV fp = f_to_parent<AX>(b, pa, c, s);
   accP.a = add(accP.a, fp.a);
   accP.l = add(accP.l, fp.l);
 }
 
-// Backward pass over the serial chain FIRST..LAST (LAST -> FIRST); the
-// chain's first body adds into (accI, accP) of its parent.
-template <int FIRST, int I, class Scr>
-G1_HD void bwd_chain(AI& IA, SV& pA, AI& accI, SV& accP, const EnvState& st, const EnvIO& io,
-                     const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
-  if constexpr (I == FIRST) {
-    bwd_body<I>(IA, pA, accI, accP, st, io, ep, cfg, scr);
-  } else {
-    AI IAp = body_inertia<I - 1>();
-    SV pAp = load_bias<I - 1>(scr);
-    bwd_body<I>(IA, pA, IAp, pAp, st, io, ep, cfg, scr);
-    bwd_chain<FIRST, I - 1>(IAp, pAp, accI, accP, st, io, ep, cfg, scr);
+G1_HD void ai_zero(AI& A) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) A.J.s[k] = A.M.s[k] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) A.H.m[k] = 0.0f;
+}
+G1_HD void ai_add(AI& A, const AI& B) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    A.J.s[k] += B.J.s[k];
+    A.M.s[k] += B.M.s[k];
   }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) A.H.m[k] += B.H.m[k];
 }
 
-template <int FIRST, int LAST, class Scr>
-G1_HD void bwd_chain_from_leaf(AI& accI, SV& accP, const EnvState& st, const EnvIO& io,
-                               const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
-  AI IA = body_inertia<LAST>();
-  SV pA = load_bias<LAST>(scr);
-  bwd_chain<FIRST, LAST>(IA, pA, accI, accP, st, io, ep, cfg, scr);
+// Backward pass over the serial chain first..last, starting from the
+// articulated inertia / bias (IA, pA) of its last body; adds the chain's
+// projection into its parent's accumulators (accI, accP).
+template <class Scr>
+G1_HD void bwd_chain(int first, int last, AI IA, SV pA, AI& accI, SV& accP, const EnvIO& io,
+                     const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
+#pragma unroll 1
+  for (int i = last; i >= first; --i) {
+    AI IAp;
+    SV pAp;
+    if (i > first) {
+      IAp = body_inertia(body(i - 1));
+      pAp = load_bias(scr, i - 1);
+    } else {
+      ai_zero(IAp);
+      pAp.a = pAp.l = mk3(0.f, 0.f, 0.f);
+    }
+    switch (body(i).axis) {
+      case 0: bwd_body<0>(i, IA, pA, IAp, pAp, io, ep, cfg, scr); break;
+      case 1: bwd_body<1>(i, IA, pA, IAp, pAp, io, ep, cfg, scr); break;
+      default: bwd_body<2>(i, IA, pA, IAp, pAp, io, ep, cfg, scr); break;
+    }
+    IA = IAp;
+    pA = pAp;
+  }
+  ai_add(accI, IA);
+  accP.a = add(accP.a, pA.a);
+  accP.l = add(accP.l, pA.l);
 }
 
 // ---------------------------------------------------------- base solve
@@ -779,40 +714,43 @@ G1_HD SV base_solve(const AI& A, const SV& pA) {
 }
 
 // --------------------------------------------------------- forward pass
-// a_i = X^-1 a_p + c_i ; qdd = (u - U.a_i) / D ; a_i += qdd S  (reference
-// src/g1_core.h:190-201), fused with the hinge's semi-implicit Euler update.
-template <int I, class Scr>
-G1_HD void fwd_body(SV& a, EnvState& st, float dt, Scr& scr) {
-  constexpr int h = I - 1, AX = axis_of(I);
+// a_i = X^-1 a_p + c_i ; qdd = u/D - (U/D).a_i ; a_i += qdd S  (reference
+// src/g1_core.h:190-201), fused with the hinge's semi-implicit Euler update
+// (reference src/g1_core.h:214,221).
+template <int AX, class Scr>
+G1_HD void fwd_body(int i, SV& a, float dt, Scr& scr) {
   constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
-  const float c = scr.template get<slot<I, 0>()>(), s = scr.template get<slot<I, 1>()>();
-  V3 t = a.l;
-  if constexpr (!p_zero<I>()) t = sub(a.l, pcross<I>(a.a));
+  const BodyC& b = body(i);
+  const float c = scr.get(hslot(i, 2)), s = scr.get(hslot(i, 3));
+  const V3 t = sub(a.l, pcross(b, a.a));
   SV an;
-  an.a = rotAT<AX>(rotTT<I>(a.a), c, s);
-  an.l = rotAT<AX>(rotTT<I>(t), c, s);
-  an.a.v[i1] += scr.template get<slot<I, 2>()>();
-  an.a.v[i2] += scr.template get<slot<I, 3>()>();
-  an.l.v[i1] += scr.template get<slot<I, 4>()>();
-  an.l.v[i2] += scr.template get<slot<I, 5>()>();
-  const float Ua0 = scr.template get<slot<I, 6>()>(), Ua1 = scr.template get<slot<I, 7>()>();
-  const float Ua2 = scr.template get<slot<I, 8>()>(), Ul0 = scr.template get<slot<I, 9>()>();
-  const float Ul1 = scr.template get<slot<I, 10>()>(), Ul2 = scr.template get<slot<I, 11>()>();
-  const float u = scr.template get<slot<I, 12>()>(), invD = scr.template get<slot<I, 13>()>();
-  const float Ua = Ua0 * an.a.v[0] + Ua1 * an.a.v[1] + Ua2 * an.a.v[2] + Ul0 * an.l.v[0] +
-                   Ul1 * an.l.v[1] + Ul2 * an.l.v[2];
-  const float qdd = (u - Ua) * invD;
+  an.a = rotAT<AX>(rotTT(b, a.a), c, s);
+  an.l = rotAT<AX>(rotTT(b, t), c, s);
+  an.a.v[i1] += scr.get(hslot(i, 4));
+  an.a.v[i2] += scr.get(hslot(i, 5));
+  an.l.v[i1] += scr.get(hslot(i, 6));
+  an.l.v[i2] += scr.get(hslot(i, 7));
+  const SV W = load_sv(scr, hslot(i, 8));  // U / D
+  const float uD = scr.get(hslot(i, 14));   // u / D
+  const float qdd = uD - (W.a.v[0] * an.a.v[0] + W.a.v[1] * an.a.v[1] + W.a.v[2] * an.a.v[2] +
+                          W.l.v[0] * an.l.v[0] + W.l.v[1] * an.l.v[1] + W.l.v[2] * an.l.v[2]);
   an.a.v[AX] += qdd;
   a = an;
-  // semi-implicit Euler (reference src/g1_core.h:214,221)
-  st.qd[h] += dt * qdd;
-  st.q[h] += dt * st.qd[h];
+  const float qd = scr.get(hslot(i, 1)) + dt * qdd;
+  scr.put(hslot(i, 1), qd);
+  scr.put(hslot(i, 0), scr.get(hslot(i, 0)) + dt * qd);
 }
 
-template <int I, int LAST, class Scr>
-G1_HD void fwd_chain(SV a, EnvState& st, float dt, Scr& scr) {
-  fwd_body<I>(a, st, dt, scr);
-  if constexpr (I < LAST) fwd_chain<I + 1, LAST>(a, st, dt, scr);
+template <class Scr>
+G1_HD void fwd_chain(int first, int last, SV& a, float dt, Scr& scr) {
+#pragma unroll 1
+  for (int i = first; i <= last; ++i) {
+    switch (body(i).axis) {
+      case 0: fwd_body<0>(i, a, dt, scr); break;
+      case 1: fwd_body<1>(i, a, dt, scr); break;
+      default: fwd_body<2>(i, a, dt, scr); break;
+    }
+  }
 }
 
 // ----------------------------------------------------------- quaternions
@@ -841,10 +779,7 @@ G1_HD void base_node(const EnvState& st, const StepConfig& cfg, FKNode& base) {
   base.g = mk3(base.R.m[6] * cfg.gravity_z, base.R.m[7] * cfg.gravity_z, base.R.m[8] * cfg.gravity_z);
 }
 
-template <int FOOT_BODY, int K0>
-G1_HD void foot_outputs(const FKNode& n, const EnvIO& io, bool last) {
-  if (!last) return;
-  constexpr int o = K0 == 0 ? 0 : 3;
+G1_HD void foot_outputs(const FKNode& n, const EnvIO& io, int o) {
   if (io.foot_pos)
 #pragma unroll
     for (int k = 0; k < 3; ++k) io.foot_pos[(o + k) * io.stride] = n.P.v[k];
@@ -855,76 +790,92 @@ G1_HD void foot_outputs(const FKNode& n, const EnvIO& io, bool last) {
   }
 }
 
+// Chains in the order each phase visits them.  FK / forward: legs, waist,
+// arms (the arms need the torso); backward: arms, waist, legs (the waist
+// needs both arms).  first, last body; the parent is the pelvis for legs and
+// waist, the torso for arms.
+G1_HD int chain_first(int c) { return c == 0 ? 1 : c == 1 ? 7 : c == 2 ? 13 : c == 3 ? 16 : 23; }
+G1_HD int chain_last(int c) { return c == 0 ? 6 : c == 1 ? 12 : c == 2 ? 15 : c == 3 ? 22 : 29; }
+
+G1_HD void sv_zero(SV& x) { x.a = x.l = mk3(0.f, 0.f, 0.f); }
+G1_HD void sv_acc(SV& x, const SV& y) {
+  x.a = add(x.a, y.a);
+  x.l = add(x.l, y.l);
+}
+
 // One substep: FK -> contacts -> PD + ABA -> integrate (reference
-// src/g1_core.h:225-232).  With last set, the foot kinematics of this
+// src/g1_core.h:225-232).  Joint angles / rates are read from and written
+// back to the scratch.  With last_sub set, the foot kinematics of this
 // substep's FK (before integration) and the contact normal forces are
-// written to io's outputs.
+// written to io's outputs.  Each phase is ONE loop over the chains so that
+// every hinge routine is instantiated once (per axis).
 template <class Scr>
 G1_HD void step(EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
-                bool last) {
-  // ---- FK + bias forces + contacts, chain by chain
+                bool last_sub) {
+  // ---- FK + bias forces + contacts: legs (world pose), waist, arms
   {
     FKNode base;
     base_node(st, cfg, base);
-    {
-      const SV pA0 = bias_force<0>(pelvis_inertia(ep.dmass), base.w, base.v, base.g);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) scr.put(kSlotPelvis + k, pA0.a.v[k]);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) scr.put(kSlotPelvis + 3 + k, pA0.l.v[k]);
-    }
-    {
-      FKNode n = base;
-      fk_chain<1, 6, true>(n, st, scr);
-      SV pA6 = load_bias<6>(scr);
-      foot_contacts<0>(n, io, last, cfg, ep.mu, pA6);
-      store_bias<6>(pA6, scr);
-      foot_outputs<6, 0>(n, io, last);
-    }
-    {
-      FKNode n = base;
-      fk_chain<7, 12, true>(n, st, scr);
-      SV pA12 = load_bias<12>(scr);
-      foot_contacts<4>(n, io, last, cfg, ep.mu, pA12);
-      store_bias<12>(pA12, scr);
-      foot_outputs<12, 4>(n, io, last);
-    }
+    store_sv(scr, kSlotPelvis, bias_force(pelvis_inertia(ep.dmass), base.w, base.v, base.g));
     FKNode torso = base;
-    fk_chain<13, 15, false>(torso, st, scr);
-    {
-      FKNode n = torso;
-      fk_chain<16, 22, false>(n, st, scr);
-    }
-    {
-      FKNode n = torso;
-      fk_chain<23, 29, false>(n, st, scr);
+#pragma unroll 1
+    for (int c = 0; c < 5; ++c) {
+      FKNode n = c < 3 ? base : torso;
+      const int first = chain_first(c), last = chain_last(c);
+      if (c < 2) {
+        fk_chain<true>(first, last, n, scr);
+        SV pA = load_bias(scr, last);
+        if (c == 0)
+          foot_contacts<0>(n, io, last_sub, cfg, ep.mu, pA);
+        else
+          foot_contacts<4>(n, io, last_sub, cfg, ep.mu, pA);
+        store_sv(scr, hslot(last, 8), pA);
+        if (last_sub) foot_outputs(n, io, c == 0 ? 0 : 3);
+      } else {
+        fk_chain<false>(first, last, n, scr);
+        if (c == 2) torso = n;
+      }
     }
   }
-  // ---- backward: arms into the torso, waist into the pelvis, then legs
-  AI acc0;
-  SV accP0;
+  // ---- backward: arms into the torso, the waist (from the torso) and the
+  // legs into the pelvis
+  AI acc0 = pelvis_inertia(ep.dmass);
+  SV accP0 = load_bias(scr, 0);
   {
-    AI acc15 = body_inertia<15>();
-    SV accP15 = load_bias<15>(scr);
-    bwd_chain_from_leaf<16, 22>(acc15, accP15, st, io, ep, cfg, scr);
-    bwd_chain_from_leaf<23, 29>(acc15, accP15, st, io, ep, cfg, scr);
-    acc0 = pelvis_inertia(ep.dmass);
-    accP0 = load_bias<0>(scr);
-    AI IA14 = body_inertia<14>();
-    SV pA14 = load_bias<14>(scr);
-    bwd_body<15>(acc15, accP15, IA14, pA14, st, io, ep, cfg, scr);
-    AI IA13 = body_inertia<13>();
-    SV pA13 = load_bias<13>(scr);
-    bwd_body<14>(IA14, pA14, IA13, pA13, st, io, ep, cfg, scr);
-    bwd_body<13>(IA13, pA13, acc0, accP0, st, io, ep, cfg, scr);
+    AI acc15 = body_inertia(body(15));
+    SV accP15 = load_bias(scr, 15);
+#pragma unroll 1
+    for (int k = 0; k < 5; ++k) {
+      const int c = k == 0 ? 3 : k == 1 ? 4 : k == 2 ? 2 : k == 3 ? 0 : 1;
+      const int first = chain_first(c), last = chain_last(c);
+      AI IA;
+      SV pA;
+      if (c == 2) {
+        IA = acc15;
+        pA = accP15;
+      } else {
+        IA = body_inertia(body(last));
+        pA = load_bias(scr, last);
+      }
+      AI contrib;
+      SV contribP;
+      ai_zero(contrib);
+      sv_zero(contribP);
+      bwd_chain(first, last, IA, pA, contrib, contribP, io, ep, cfg, scr);
+      if (c >= 3) {
+        ai_add(acc15, contrib);
+        sv_acc(accP15, contribP);
+      } else {
+        ai_add(acc0, contrib);
+        sv_acc(accP0, contribP);
+      }
+    }
   }
-  bwd_chain_from_leaf<1, 6>(acc0, accP0, st, io, ep, cfg, scr);
-  bwd_chain_from_leaf<7, 12>(acc0, accP0, st, io, ep, cfg, scr);
-  // ---- base acceleration and forward pass (fused with integration)
+  // ---- base acceleration
   const SV a0 = base_solve(acc0, accP0);
   const float dt = cfg.dt;
-  // base: MuJoCo free-joint qacc (world linear incl. w x v, body angular);
-  // uses the pre-integration base frame, rebuilt from the unchanged state
+  // base velocity: MuJoCo free-joint qacc (world linear incl. w x v, body
+  // angular) from the pre-integration base frame
   {
     FKNode base;
     base_node(st, cfg, base);
@@ -934,20 +885,20 @@ G1_HD void step(EnvState& st, const EnvIO& io, const EnvParams& ep, const StepCo
 #pragma unroll
     for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
   }
-  fwd_chain<1, 6>(a0, st, dt, scr);
-  fwd_chain<7, 12>(a0, st, dt, scr);
+  // ---- forward pass, fused with the hinge integration: legs, waist, arms
   {
-    SV a = a0;
-    fwd_body<13>(a, st, dt, scr);
-    fwd_body<14>(a, st, dt, scr);
-    fwd_body<15>(a, st, dt, scr);
-    fwd_chain<16, 22>(a, st, dt, scr);
-    fwd_chain<23, 29>(a, st, dt, scr);
+    SV a15 = a0;
+#pragma unroll 1
+    for (int c = 0; c < 5; ++c) {
+      SV a = c < 3 ? a0 : a15;
+      fwd_chain(chain_first(c), chain_last(c), a, dt, scr);
+      if (c == 2) a15 = a;
+    }
   }
   // ---- base position and orientation (semi-implicit Euler)
-  {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
+  for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
+  {
     // q <- q (x) exp(w dt / 2), renormalised (reference src/spatial.h:73-79)
     const float wx = st.wb[0], wy = st.wb[1], wz = st.wb[2];
     const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
@@ -965,6 +916,24 @@ G1_HD void step(EnvState& st, const EnvIO& io, const EnvParams& ep, const StepCo
       r[3] = a[0] * dq[3] + a[1] * dq[2] - a[2] * dq[1] + a[3] * dq[0];
       quat_normalized(r, st.quat);
     }
+  }
+}
+
+// Joint angles / rates between the SoA state arrays and the scratch.
+template <class Scr>
+G1_HD void load_joints(const float* qpos, const float* qvel, size_t stride, Scr& scr) {
+#pragma unroll 1
+  for (int h = 0; h < kNJ; ++h) {
+    scr.put(hslot(h + 1, 0), qpos[(7 + h) * stride]);
+    scr.put(hslot(h + 1, 1), qvel[(6 + h) * stride]);
+  }
+}
+template <class Scr>
+G1_HD void store_joints(float* qpos, float* qvel, size_t stride, Scr& scr) {
+#pragma unroll 1
+  for (int h = 0; h < kNJ; ++h) {
+    qpos[(7 + h) * stride] = scr.get(hslot(h + 1, 0));
+    qvel[(6 + h) * stride] = scr.get(hslot(h + 1, 1));
   }
 }
 
