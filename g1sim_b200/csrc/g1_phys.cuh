@@ -65,6 +65,10 @@ struct BodyC {
   float m;
   float kp, kv, lim, lo, hi, arm, damp;  // servo and joint (hinges only)
   int axis, ident;
+  // extended precision for the leg world-pose chain: p = p + p_lo, and the
+  // tree rotation as a rotation about y by an angle with cos / sin = hi + lo
+  float p_lo[3];
+  float ty_c, ty_c_lo, ty_s, ty_s_lo;
 };
 struct ModelC {
   BodyC b[kNB];
@@ -82,6 +86,11 @@ constexpr ModelC make_model() {
     for (int k = 0; k < 9; ++k) b.H[k] = (float)g1m_sp_inertia[16 * i + 6 + k];
     b.m = (float)g1m_sp_inertia[16 * i + 15];
     b.ident = g1m_tree_ident[i];
+    for (int k = 0; k < 3; ++k) b.p_lo[k] = (float)(g1m_tree_pos[3 * i + k] - (double)b.p[k]);
+    b.ty_c = (float)g1m_tree_ycs[2 * i];
+    b.ty_c_lo = (float)(g1m_tree_ycs[2 * i] - (double)b.ty_c);
+    b.ty_s = (float)g1m_tree_ycs[2 * i + 1];
+    b.ty_s_lo = (float)(g1m_tree_ycs[2 * i + 1] - (double)b.ty_s);
     if (i > 0) {
       const int h = i - 1;
       b.kp = (float)g1m_act_kp[h];
@@ -163,6 +172,106 @@ struct AI {
 struct SV {
   V3 a, l;
 };
+
+// ---------------------------------------------- float-float arithmetic
+// A value hi + lo held as two floats (unevaluated sum), with the error-free
+// transformations TwoSum (Knuth), FastTwoSum (Dekker, |a| >= |b|) and the
+// FMA-based TwoProd.  Used for the leg world-pose chain, where the contact
+// depth is the difference of two ~0.8 m quantities and kn = 2e4 N/m turns
+// FP32 rounding of positions into newton-level force errors.
+struct F2 {
+  float hi, lo;
+};
+G1_HD F2 f2(float x) { return F2{x, 0.0f}; }
+G1_HD F2 fast_two_sum(float a, float b) {
+  const float s = a + b;
+  return F2{s, b - (s - a)};
+}
+G1_HD F2 two_sum(float a, float b) {
+  const float s = a + b;
+  const float bb = s - a;
+  return F2{s, (a - (s - bb)) + (b - bb)};
+}
+G1_HD F2 two_prod(float a, float b) {
+  const float p = a * b;
+  return F2{p, fmaf(a, b, -p)};
+}
+G1_HD F2 ff_add(F2 x, F2 y) {
+  const F2 t = two_sum(x.hi, y.hi);
+  return fast_two_sum(t.hi, t.lo + (x.lo + y.lo));
+}
+G1_HD F2 ff_sub(F2 x, F2 y) { return ff_add(x, F2{-y.hi, -y.lo}); }
+G1_HD F2 ff_mul(F2 x, F2 y) {
+  const F2 p = two_prod(x.hi, y.hi);
+  return fast_two_sum(p.hi, fmaf(x.hi, y.lo, fmaf(x.lo, y.hi, p.lo)));
+}
+G1_HD F2 ff_mul_f(F2 x, float y) {
+  const F2 p = two_prod(x.hi, y);
+  return fast_two_sum(p.hi, fmaf(x.lo, y, p.lo));
+}
+
+// sin / cos of k / 32 rad, hi + lo, |k| <= G1M_SINCOS_K.
+struct SinCosTab {
+  float v[2 * G1M_SINCOS_K + 1][4];  // sin hi, sin lo, cos hi, cos lo
+};
+constexpr SinCosTab make_sincos_tab() {
+  SinCosTab t{};
+  for (int k = 0; k < 2 * G1M_SINCOS_K + 1; ++k) {
+    const double sn = g1m_sincos_tab[2 * k], cs = g1m_sincos_tab[2 * k + 1];
+    t.v[k][0] = (float)sn;
+    t.v[k][1] = (float)(sn - (double)(float)sn);
+    t.v[k][2] = (float)cs;
+    t.v[k][3] = (float)(cs - (double)(float)cs);
+  }
+  return t;
+}
+#if defined(__CUDACC__)
+static __device__ SinCosTab d_sincos_tab = make_sincos_tab();
+#endif
+static constexpr SinCosTab kSinCosTab = make_sincos_tab();
+
+// sin and cos of a float angle to ~1e-14: q = k/32 + r with |r| <= 1/64
+// (r is exact: Sterbenz), tabulated sin / cos (k/32), Taylor series of
+// sin r and cos r to r^5 / r^6 (truncation < 1e-16), angle addition in
+// float-float (the table-driven method of P. T. P. Tang).
+G1_HD void sincos_ff(float q, F2& sn, F2& cs) {
+  const float kf = rintf(q * 32.0f);
+  if (!(fabsf(kf) <= (float)G1M_SINCOS_K)) {  // outside the table (or NaN)
+    float s, c;
+    sincosf(q, &s, &c);
+    sn = f2(s);
+    cs = f2(c);
+    return;
+  }
+  const float r = q - kf * (1.0f / 32.0f);
+  const int k = (int)kf + G1M_SINCOS_K;
+#if defined(__CUDA_ARCH__)
+  const float4 e = __ldg(reinterpret_cast<const float4*>(&d_sincos_tab.v[k][0]));
+  const F2 S{e.x, e.y}, C{e.z, e.w};
+#else
+  const F2 S{kSinCosTab.v[k][0], kSinCosTab.v[k][1]}, C{kSinCosTab.v[k][2], kSinCosTab.v[k][3]};
+#endif
+  const float r2 = r * r;
+  const F2 sr = fast_two_sum(r, r * r2 * fmaf(r2, 1.0f / 120.0f, -1.0f / 6.0f));
+  const F2 rr = two_prod(r, r);
+  const F2 c1 = fast_two_sum(1.0f, -0.5f * rr.hi);
+  const F2 cr = fast_two_sum(c1.hi, (c1.lo - 0.5f * rr.lo) + rr.hi * rr.hi * fmaf(rr.hi, -1.0f / 720.0f, 1.0f / 24.0f));
+  sn = ff_add(ff_mul(S, cr), ff_mul(C, sr));
+  cs = ff_sub(ff_mul(C, cr), ff_mul(S, sr));
+}
+
+// Right-multiply a float-float 3x3 by a rotation about basis axis AX with
+// (c, s): columns i1 <- c i1 + s i2, i2 <- c i2 - s i1.
+template <int AX>
+G1_HD void ff_rot_cols(F2* R, F2 c, F2 s) {
+  constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const F2 x = R[3 * a + i1], y = R[3 * a + i2];
+    R[3 * a + i1] = ff_add(ff_mul(c, x), ff_mul(s, y));
+    R[3 * a + i2] = ff_sub(ff_mul(c, y), ff_mul(s, x));
+  }
+}
 
 // ------------------------------------------------- joint axis rotation (A)
 // A rotates by q about basis axis AX: it mixes coordinates i=(AX+1)%3 and
@@ -352,11 +461,13 @@ struct EnvParams {
   float mu, dmass, kp_scale, kd_scale;
 };
 
-// Running FK values of one body: body-frame twist, gravity, world pose (legs only).
+// Running FK values of one body: body-frame twist, gravity, and (legs only)
+// the world pose in float-float (Rf, Pf) with its float rounding (R, P).
 struct FKNode {
   V3 w, v, g;
   M3 R;
   V3 P;
+  F2 Rf[9], Pf[3];
 };
 
 template <class Scr>
@@ -388,7 +499,14 @@ G1_HD void fk_body(int i, FKNode& n, Scr& scr) {
   const BodyC& b = body(i);
   const float q = scr.get(hslot(i, 0)), qd = scr.get(hslot(i, 1));
   float s, c;
-  sincosf(q, &s, &c);
+  F2 sf, cf;
+  if constexpr (kWorld) {
+    sincos_ff(q, sf, cf);
+    s = sf.hi;
+    c = cf.hi;
+  } else {
+    sincosf(q, &s, &c);
+  }
   scr.put(hslot(i, 2), c);
   scr.put(hslot(i, 3), s);
   // parent -> child: x_c = A^T T^T x_p ;  v.l uses v_p - p x w_p
@@ -398,23 +516,20 @@ G1_HD void fk_body(int i, FKNode& n, Scr& scr) {
   const V3 g = rotAT<AX>(rotTT(b, n.g), c, s);
   w.v[AX] += qd;
   if constexpr (kWorld) {
-    // R_i = R_p T A ; P_i = P_p + R_p p
-    M3 RT = n.R;
-    if (!b.ident) {
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int bb = 0; bb < 3; ++bb)
-          RT.m[3 * a + bb] = n.R.m[3 * a] * b.T[bb] + n.R.m[3 * a + 1] * b.T[3 + bb] + n.R.m[3 * a + 2] * b.T[6 + bb];
-    }
-    M3 R = RT;
+    // world pose in float-float: P_i = P_p + R_p p ; R_i = R_p T A
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      R.m[3 * a + i1] = c * RT.m[3 * a + i1] + s * RT.m[3 * a + i2];
-      R.m[3 * a + i2] = c * RT.m[3 * a + i2] - s * RT.m[3 * a + i1];
+      F2 acc = n.Pf[a];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc = ff_add(acc, ff_mul(n.Rf[3 * a + k], F2{b.p[k], b.p_lo[k]}));
+      n.Pf[a] = acc;
     }
-    n.P = add(n.P, mv(n.R, mk3(b.p[0], b.p[1], b.p[2])));
-    n.R = R;
+    if (!b.ident) ff_rot_cols<1>(n.Rf, F2{b.ty_c, b.ty_c_lo}, F2{b.ty_s, b.ty_s_lo});
+    ff_rot_cols<AX>(n.Rf, cf, sf);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) n.R.m[k] = n.Rf[k].hi;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) n.P.v[k] = n.Pf[k].hi;
   }
   n.w = w;
   n.v = v;
@@ -460,8 +575,14 @@ G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const Step
   for (int k = K0; k < K0 + 4; ++k) {
     const V3 r = mk3(M.contact_pos[3 * k], M.contact_pos[3 * k + 1], M.contact_pos[3 * k + 2]);
     const V3 rw = mv(n.R, r);
-    const float px = n.P.v[0] + rw.v[0], py = n.P.v[1] + rw.v[1], pz = n.P.v[2] + rw.v[2];
-    const float depth = radius - pz;
+    // sphere centre in float-float: P + R r
+    F2 pc[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      pc[a] = ff_add(ff_add(n.Pf[a], ff_mul_f(n.Rf[3 * a], r.v[0])),
+                     ff_add(ff_mul_f(n.Rf[3 * a + 1], r.v[1]), ff_mul_f(n.Rf[3 * a + 2], r.v[2])));
+    const float px = pc[0].hi, py = pc[1].hi;
+    const float depth = (radius - pc[2].hi) - pc[2].lo;
     const bool in = depth > 0.0f;
     const V3 vp = add(vo, crs(ww, rw));
     float fn = cfg.contact_kn * depth - cfg.contact_dn * vp.v[2];
@@ -470,15 +591,17 @@ G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const Step
     const bool fresh = ax >= kAnchorFree;
     ax = fresh ? px : ax;
     ay = fresh ? py : ay;
-    float ftx = -cfg.contact_kt * (px - ax) - cfg.contact_dt * vp.v[0];
-    float fty = -cfg.contact_kt * (py - ay) - cfg.contact_dt * vp.v[1];
+    // spring stretch (p - anchor) with the low part of p kept
+    const float dx = (px - ax) + pc[0].lo, dy = (py - ay) + pc[1].lo;
+    float ftx = -cfg.contact_kt * dx - cfg.contact_dt * vp.v[0];
+    float fty = -cfg.contact_kt * dy - cfg.contact_dt * vp.v[1];
     const float ftn = sqrtf(ftx * ftx + fty * fty), fmax = mu * fn;
     if (ftn > fmax) {
       const float sc = fmax / (ftn + 1e-12f);
       ftx *= sc;
       fty *= sc;
-      ax = px + ftx * inv_kt;
-      ay = py + fty * inv_kt;
+      ax = px + (ftx * inv_kt + pc[0].lo);
+      ay = py + (fty * inv_kt + pc[1].lo);
     }
     if (in) {
       anchor[(2 * k) * sd] = ax;
@@ -779,6 +902,32 @@ G1_HD void base_node(const EnvState& st, const StepConfig& cfg, FKNode& base) {
   base.g = mk3(base.R.m[6] * cfg.gravity_z, base.R.m[7] * cfg.gravity_z, base.R.m[8] * cfg.gravity_z);
 }
 
+// Base world pose in float-float: R(q) of the (not exactly unit) stored
+// quaternion, R = I + 2/|q|^2 [..] (the reference normalises, then converts,
+// src/g1_core.h:31-32; same matrix), and the position.
+G1_HD void base_pose_ff(const EnvState& st, FKNode& n) {
+  const float w = st.quat[0], x = st.quat[1], y = st.quat[2], z = st.quat[3];
+  const F2 ww = two_prod(w, w), xx = two_prod(x, x), yy = two_prod(y, y), zz = two_prod(z, z);
+  const F2 n2 = ff_add(ff_add(ww, xx), ff_add(yy, zz));
+  // 2 / |q|^2: float reciprocal refined by one Newton step in float-float
+  const float y0 = 1.0f / n2.hi;
+  const F2 e = ff_sub(f2(1.0f), ff_mul_f(n2, y0));
+  const F2 inv2 = fast_two_sum(2.0f * y0, 2.0f * y0 * e.hi);
+  const F2 xy = two_prod(x, y), xz = two_prod(x, z), yz = two_prod(y, z);
+  const F2 wx = two_prod(w, x), wy = two_prod(w, y), wz = two_prod(w, z);
+  n.Rf[0] = ff_sub(f2(1.0f), ff_mul(inv2, ff_add(yy, zz)));
+  n.Rf[1] = ff_mul(inv2, ff_sub(xy, wz));
+  n.Rf[2] = ff_mul(inv2, ff_add(xz, wy));
+  n.Rf[3] = ff_mul(inv2, ff_add(xy, wz));
+  n.Rf[4] = ff_sub(f2(1.0f), ff_mul(inv2, ff_add(xx, zz)));
+  n.Rf[5] = ff_mul(inv2, ff_sub(yz, wx));
+  n.Rf[6] = ff_mul(inv2, ff_sub(xz, wy));
+  n.Rf[7] = ff_mul(inv2, ff_add(yz, wx));
+  n.Rf[8] = ff_sub(f2(1.0f), ff_mul(inv2, ff_add(xx, yy)));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) n.Pf[k] = f2(st.pos[k]);
+}
+
 G1_HD void foot_outputs(const FKNode& n, const EnvIO& io, int o) {
   if (io.foot_pos)
 #pragma unroll
@@ -816,6 +965,7 @@ G1_HD void step(EnvState& st, const EnvIO& io, const EnvParams& ep, const StepCo
   {
     FKNode base;
     base_node(st, cfg, base);
+    base_pose_ff(st, base);
     store_sv(scr, kSlotPelvis, bias_force(pelvis_inertia(ep.dmass), base.w, base.v, base.g));
     FKNode torso = base;
 #pragma unroll 1

@@ -38,6 +38,7 @@ PKG = os.path.dirname(HERE)
 # although the foot class of model/g1_raw.xml says friction="0.6".  The value
 # that the reference's code actually uses is the one kept here.
 CONTACT_MU = 1.0
+SINCOS_K = 202
 
 
 def _vec(s, n=None):
@@ -299,13 +300,35 @@ def derived(data):
         # J (xx, yy, zz, xy, xz, yz), H row-major, M = m I
         sp_inertia.append([J[0, 0], J[1, 1], J[2, 2], J[0, 1], J[0, 2], J[1, 2]]
                           + list(H.reshape(-1)) + [m])
+    # leg bodies: their tree rotation must be identity or a pure rotation
+    # about y (the device composes it in extended precision as a (cos, sin)
+    # pair); record cos / sin of that rotation
+    tree_ycs = []
+    for i in range(nb):
+        R = np.asarray(tree_rot[i]).reshape(3, 3)
+        if tree_ident[i]:
+            tree_ycs.append([1.0, 0.0])
+            continue
+        is_y = abs(R[1, 1] - 1) < 1e-15 and abs(R[0, 1]) < 1e-15 and abs(R[1, 0]) < 1e-15 \
+            and abs(R[1, 2]) < 1e-15 and abs(R[2, 1]) < 1e-15
+        leg = 1 <= i <= 12
+        assert is_y or not leg, f"leg body {i}: tree rotation is not about y"
+        q = data["tree_quat"][i]
+        ang = 2.0 * math.atan2(q[2], q[0]) if is_y else 0.0
+        tree_ycs.append([math.cos(ang), math.sin(ang)] if is_y else [1.0, 0.0])
     for h, ax in enumerate(data["jnt_axis"]):
         nz = [k for k in range(3) if ax[k] != 0.0]
         assert len(nz) == 1 and ax[nz[0]] == 1.0, "hinge axes must be +x, +y or +z"
         assert data["jnt_anchor"][h] == [0.0, 0.0, 0.0], "hinge anchors must be at the body origin"
         axis_idx.append(nz[0])
+    # sin / cos of k / 32 rad for |k| <= 202 (|angle| <= 6.3125), in double, for
+    # the device's extended-precision sin/cos (angle addition + short Taylor).
+    sincos_tab = []
+    for k in range(-SINCOS_K, SINCOS_K + 1):
+        a = k / 32.0
+        sincos_tab.append([math.sin(a), math.cos(a)])
     return dict(tree_rot=tree_rot, tree_ident=tree_ident, sp_inertia=sp_inertia,
-                axis_idx=axis_idx)
+                axis_idx=axis_idx, sincos_tab=sincos_tab, tree_ycs=tree_ycs)
 
 
 def emit_derived_h(data, der, path):
@@ -332,6 +355,9 @@ def emit_derived_h(data, der, path):
         f.write(arr("g1m_tree_ident", der["tree_ident"], "int"))
         f.write(arr("g1m_sp_inertia", der["sp_inertia"]))
         f.write(arr("g1m_axis_idx", der["axis_idx"], "int"))
+        f.write(arr("g1m_tree_ycs", der["tree_ycs"]))
+        f.write(f"#define G1M_SINCOS_K {SINCOS_K}\n")
+        f.write(arr("g1m_sincos_tab", der["sincos_tab"]))
         f.write("\n#endif  // G1M_MODEL_DERIVED_H\n")
 
 
