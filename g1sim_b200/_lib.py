@@ -46,8 +46,8 @@ def lib():
     L.g1b_last_error.restype = C.c_char_p
     L.g1b_step.argtypes = [C.c_int, C.c_int, C.POINTER(Config)] + [_vp] * 12
     L.g1b_rollout.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(Config), C.POINTER(RolloutParams)] + [_vp] * 11
-    L.g1b_set_launch.argtypes = [C.c_int, C.c_int]
-    L.g1b_get_launch.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.g1b_set_launch.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.g1b_get_launch.argtypes = [C.POINTER(C.c_int)] * 3
     L.g1b_autotune.argtypes = [C.c_int, C.c_int, _vp, C.POINTER(C.c_float)]
     L.g1b_ffma_peak.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     _lib = L
@@ -66,6 +66,25 @@ def default_config(dt=None):
     if dt is not None:
         c.dt = dt
     return c
+
+
+def set_launch(mapping, block, blocks_per_sm=0):
+    """Launch shape of the step kernels (mapping 0: thread per env, 1: two threads per env)."""
+    check(lib().g1b_set_launch(int(mapping), int(block), int(blocks_per_sm)), "g1b_set_launch")
+
+
+def autotune(nenv, nsub=10, stream=None):
+    """Time every launch shape on this device for nenv envs x nsub substeps; keep the fastest.
+    Returns (mapping, block, blocks_per_sm, best_ms)."""
+    best = C.c_float()
+    check(lib().g1b_autotune(int(nenv), int(nsub), stream, C.byref(best)), "g1b_autotune")
+    return get_launch() + (best.value,)
+
+
+def get_launch():
+    v = [C.c_int() for _ in range(3)]
+    check(lib().g1b_get_launch(*[C.byref(x) for x in v]), "g1b_get_launch")
+    return tuple(x.value for x in v)
 
 
 def last_error():

@@ -41,7 +41,7 @@ struct SmemScratch {
 };
 
 template <int BLOCK>
-constexpr size_t smem_bytes() { return (size_t)kNumSlots * BLOCK * sizeof(float); }
+constexpr size_t smem_bytes() { return (size_t)kNumSlotsSingle * BLOCK * sizeof(float); }
 
 struct StateArgs {
   int nenv;
@@ -159,12 +159,13 @@ __device__ __forceinline__ float draw_target(unsigned seed, int e, int step, flo
   const float span = __fmul_rn(frac, __fsub_rn(hi, lo));
   return __fadd_rn(stand, __fmul_rn(r, span));
 }
-// writes the env's targets into its ctrl column (read back by the substeps)
-template <int J>
+// writes the env's targets of joints J..J1-1 into its ctrl column (read back
+// by the substeps)
+template <int J, int J1 = kNU>
 __device__ __forceinline__ void draw_targets(float* ct, size_t stride, unsigned seed, int e, int step,
                                              float frac) {
   ct[J * stride] = draw_target<J>(seed, e, step, frac);
-  if constexpr (J + 1 < kNU) draw_targets<J + 1>(ct, stride, seed, e, step, frac);
+  if constexpr (J + 1 < J1) draw_targets<J + 1, J1>(ct, stride, seed, e, step, frac);
 }
 
 template <int BLOCK>
@@ -209,6 +210,158 @@ __global__ void __launch_bounds__(BLOCK) rollout_kernel(StateArgs a, float* ctrl
   }
 }
 
+
+// ------------------------------------------------------- split mapping
+// Two threads per env: threads [0, ENVS) run the lower body (pelvis, legs,
+// contacts, base solve and base integration), threads [ENVS, 2 ENVS) the
+// upper body (waist, arms) of env tile * ENVS + (tid % ENVS).  Both halves
+// use the env's slot column of the shared scratch and exchange, per
+// substep, the upper body's projection into the pelvis, the base
+// acceleration and the base state (three block barriers).  kRollout: the
+// decimated rollout (target redraw, reset); otherwise ninner substeps.
+template <int ENVS, bool kRollout>
+__global__ void __launch_bounds__(2 * ENVS) split_kernel(StateArgs a, float* ctrl, int* reset_count,
+                                                         int nouter, int ninner, StepConfig cfg,
+                                                         RolloutParams rp) {
+  extern __shared__ float sm[];
+  const int role = threadIdx.x >= ENVS ? 1 : 0;  // warp-uniform (ENVS is a multiple of 32)
+  const int le = threadIdx.x - role * ENVS;
+  SmemScratch<ENVS> scr{sm + le};
+  const int n = a.nenv;
+  const size_t sd = (size_t)n;
+  const int ntiles = (n + ENVS - 1) / ENVS;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e = tile * ENVS + le;
+    const bool act = e < n;
+    EnvState st;
+    EnvIO io;
+    EnvParams ep;
+    if (act) {
+      io = env_io(a, ctrl, e);
+      ep = load_params(a, e);
+      if (role == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) st.pos[k] = a.qpos[k * sd + e];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) st.quat[k] = a.qpos[(3 + k) * sd + e];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) st.vw[k] = a.qvel[k * sd + e];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) st.wb[k] = a.qvel[(3 + k) * sd + e];
+        load_joints(a.qpos + e, a.qvel + e, sd, scr, 1, 12);
+        store_base(scr, st);
+      } else {
+        load_joints(a.qpos + e, a.qvel + e, sd, scr, 13, kNJ);
+      }
+    }
+    __syncthreads();
+    int resets = 0;
+    for (int k = 0; k < nouter; ++k) {
+      const int stp = rp.step0 + k;
+      if (kRollout && act && rp.redraw) {
+        if (role == 0)
+          draw_targets<0, 12>(ctrl + e, sd, rp.seed, e, stp, rp.target_frac);
+        else
+          draw_targets<12, kNU>(ctrl + e, sd, rp.seed, e, stp, rp.target_frac);
+      }
+      for (int s = 0; s < ninner; ++s) {
+        const bool last_sub = (k == nouter - 1) && (s == ninner - 1);
+        AI acc0;
+        SV accP0;
+        EnvState su;  // upper half: base state at the start of the substep
+        if (act) {
+          if (role == 0) {
+            fk_lower(st, io, ep, cfg, scr, last_sub);
+            bwd_lower(st, io, ep, cfg, scr, acc0, accP0);
+          } else {
+            load_base(scr, su);
+            fk_upper(su, cfg, scr);
+            AI up;
+            SV upP;
+            bwd_upper(io, ep, cfg, scr, up, upP);
+            store_ai(scr, kXUp, up, upP);
+          }
+        }
+        __syncthreads();
+        SV a0;
+        if (act && role == 0) {
+          AI up;
+          SV upP;
+          load_ai(scr, kXUp, up, upP);
+          ai_add(acc0, up);
+          sv_acc(accP0, upP);
+          a0 = base_solve(acc0, accP0);
+          store_sv(scr, kXA0, a0);
+        }
+        __syncthreads();
+        if (act) {
+          if (role == 1) {
+            fwd_upper(su, load_sv(scr, kXA0), cfg, scr);
+          } else {
+            fwd_lower_and_base(st, a0, cfg, scr);
+            store_base(scr, st);
+          }
+        }
+        __syncthreads();
+      }
+      if (kRollout) {
+        if (act && role == 0) {
+          const bool rs = st.pos[2] < rp.reset_z;
+          if (rs) {
+            const float u = uniform24(rp.seed ^ 0x5bd1e995u, (unsigned)e, (unsigned)stp);
+            const float z0 = __fadd_rn(rp.z0_lo, __fmul_rn(u, __fsub_rn(rp.z0_hi, rp.z0_lo)));
+#pragma unroll
+            for (int i = 0; i < 3; ++i) st.pos[i] = model().stand[i];
+            st.pos[2] = z0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) st.quat[i] = model().stand[3 + i];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) st.vw[i] = st.wb[i] = 0.0f;
+#pragma unroll 1
+            for (int i = 1; i <= 12; ++i) {
+              scr.put(hslot(i, 0), model().stand[6 + i]);
+              scr.put(hslot(i, 1), 0.0f);
+            }
+#pragma unroll
+            for (int i = 0; i < 2 * kNC; ++i) a.anchor[(size_t)i * sd + e] = kAnchorFree;
+            store_base(scr, st);
+            ++resets;
+          }
+          scr.put(kXReset, rs ? 1.0f : 0.0f);
+        }
+        __syncthreads();
+        if (act && role == 1 && scr.get(kXReset) != 0.0f) {
+#pragma unroll 1
+          for (int i = 13; i <= kNJ; ++i) {
+            scr.put(hslot(i, 0), model().stand[6 + i]);
+            scr.put(hslot(i, 1), 0.0f);
+          }
+        }
+      }
+    }
+    if (act) {
+      if (role == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.qpos[k * sd + e] = st.pos[k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a.qpos[(3 + k) * sd + e] = st.quat[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.qvel[k * sd + e] = st.vw[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.qvel[(3 + k) * sd + e] = st.wb[k];
+        store_joints(a.qpos + e, a.qvel + e, sd, scr, 1, 12);
+        if (kRollout && reset_count) reset_count[e] += resets;
+      } else {
+        store_joints(a.qpos + e, a.qvel + e, sd, scr, 13, kNJ);
+      }
+    }
+    __syncthreads();  // the next tile reuses the scratch
+  }
+}
+
+template <int ENVS>
+constexpr size_t smem_bytes_split() { return (size_t)kNumSlots * ENVS * sizeof(float); }
+
 // ------------------------------------------------------------- reset
 // reference src/g1_kernel.cu:85-103: stand keyframe, +drop on z, joint noise
 // noise * (2u - 1) from the per-env hash stream, qvel = 0, anchors free.
@@ -252,6 +405,17 @@ __global__ void __launch_bounds__(256) ffma_kernel(int iters, float a, float b) 
   if (s == 1234.5f) g_ffma_sink[blockIdx.x & 1023] = s;  // keeps the chains live
 }
 
+// Stand pose, zero velocity, free anchors, stand targets (autotuner state).
+__global__ void init_stand_kernel(int nenv, float* qpos, float* qvel, float* anchor, float* ctrl) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nenv) return;
+  const size_t n = (size_t)nenv;
+  for (int i = 0; i < kNQ; ++i) qpos[i * n + e] = model().stand[i];
+  for (int i = 0; i < kNV; ++i) qvel[i * n + e] = 0.0f;
+  for (int i = 0; i < 2 * kNC; ++i) anchor[i * n + e] = kAnchorFree;
+  for (int i = 0; i < kNU; ++i) ctrl[i * n + e] = model().stand[7 + i];
+}
+
 }  // namespace g1b
 
 // =================================================================== host
@@ -261,6 +425,7 @@ namespace {
 
 thread_local char g_err[512] = "";
 std::mutex g_mu;
+int g_mapping = 1;  // two threads per env
 int g_block = 128;
 int g_blocks_per_sm = 0;
 
@@ -337,63 +502,78 @@ cudaError_t prepare(K kernel, size_t smem) {
   return e;
 }
 
-template <int BLOCK>
-int launch_step(const StateArgs& a, const float* ctrl, int nsub, const StepConfig& cfg,
-                cudaStream_t stream, int blocks_per_sm) {
-  constexpr size_t smem = smem_bytes<BLOCK>();
-  auto k = step_kernel<BLOCK>;
-  cudaError_t e = prepare<0, BLOCK>(k, smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(step)");
-  const int grid = grid_for<0, BLOCK>(k, BLOCK, smem, a.nenv, blocks_per_sm);
-  k<<<grid, BLOCK, smem, stream>>>(a, ctrl, nsub, cfg);
+// Launch of one kernel instance: attribute opt-in, resident-capped grid.
+template <int KIND, int BLOCK, class K, class... Args>
+int launch(K kernel, int threads, size_t smem, int nwork, int items_per_block, int bps, cudaStream_t stream,
+           const char* what, Args... args) {
+  cudaError_t e = prepare<KIND, BLOCK>(kernel, smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  const int need = (nwork + items_per_block - 1) / items_per_block;
+  int grid = grid_for<KIND, BLOCK>(kernel, threads, smem, need * threads, bps);
+  if (grid > need) grid = need;
+  kernel<<<grid, threads, smem, stream>>>(args...);
   e = cudaGetLastError();
-  return e == cudaSuccess ? 0 : cuda_fail(e, "step_kernel launch");
+  return e == cudaSuccess ? 0 : cuda_fail(e, what);
 }
 
+// One entry per launch shape: mapping 0 = one thread per env (BLOCK threads,
+// BLOCK envs per block), mapping 1 = two threads per env (BLOCK envs,
+// 2 * BLOCK threads per block).
 template <int BLOCK>
-int launch_rollout(const StateArgs& a, float* ctrl, int* rc, int npolicy, int decim,
-                   const StepConfig& cfg, const RolloutParams& rp, cudaStream_t stream,
-                   int blocks_per_sm) {
+int run_single(bool rollout, const StateArgs& a, float* ctrl, int* rc, int nouter, int ninner,
+               const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s, int bps) {
   constexpr size_t smem = smem_bytes<BLOCK>();
-  auto k = rollout_kernel<BLOCK>;
-  cudaError_t e = prepare<1, BLOCK>(k, smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(rollout)");
-  const int grid = grid_for<1, BLOCK>(k, BLOCK, smem, a.nenv, blocks_per_sm);
-  k<<<grid, BLOCK, smem, stream>>>(a, ctrl, rc, npolicy, decim, cfg, rp);
-  e = cudaGetLastError();
-  return e == cudaSuccess ? 0 : cuda_fail(e, "rollout_kernel launch");
+  if (rollout)
+    return launch<1, BLOCK>(rollout_kernel<BLOCK>, BLOCK, smem, a.nenv, BLOCK, bps, s, "rollout_kernel", a, ctrl, rc,
+                            nouter, ninner, cfg, rp);
+  return launch<0, BLOCK>(step_kernel<BLOCK>, BLOCK, smem, a.nenv, BLOCK, bps, s, "step_kernel", a,
+                          (const float*)ctrl, ninner, cfg);
+}
+template <int ENVS>
+int run_split(bool rollout, const StateArgs& a, float* ctrl, int* rc, int nouter, int ninner,
+              const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s, int bps) {
+  constexpr size_t smem = smem_bytes_split<ENVS>();
+  if (rollout)
+    return launch<3, ENVS>(split_kernel<ENVS, true>, 2 * ENVS, smem, a.nenv, ENVS, bps, s, "split_kernel", a, ctrl,
+                           rc, nouter, ninner, cfg, rp);
+  return launch<2, ENVS>(split_kernel<ENVS, false>, 2 * ENVS, smem, a.nenv, ENVS, bps, s, "split_kernel", a, ctrl,
+                         rc, 1, ninner, cfg, rp);
 }
 
-int dispatch_step(const StateArgs& a, const float* ctrl, int nsub, const StepConfig& cfg,
-                  cudaStream_t s) {
-  int block, bps;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    block = g_block;
-    bps = g_blocks_per_sm;
+struct LaunchShape {
+  int mapping, block, bps;
+};
+LaunchShape current_shape() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return LaunchShape{g_mapping, g_block, g_blocks_per_sm};
+}
+
+int dispatch(const LaunchShape& L, bool rollout, const StateArgs& a, float* ctrl, int* rc, int nouter,
+             int ninner, const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s) {
+  if (L.mapping == 1) {
+    switch (L.block) {
+      case 32: return run_split<32>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+      case 64: return run_split<64>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+      case 96: return run_split<96>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+      default: return run_split<128>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+    }
   }
-  switch (block) {
-    case 32: return launch_step<32>(a, ctrl, nsub, cfg, s, bps);
-    case 64: return launch_step<64>(a, ctrl, nsub, cfg, s, bps);
-    case 96: return launch_step<96>(a, ctrl, nsub, cfg, s, bps);
-    default: return launch_step<128>(a, ctrl, nsub, cfg, s, bps);
+  switch (L.block) {
+    case 32: return run_single<32>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+    case 64: return run_single<64>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+    case 96: return run_single<96>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+    default: return run_single<128>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
   }
 }
 
-int dispatch_rollout(const StateArgs& a, float* ctrl, int* rc, int npolicy, int decim,
-                     const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s) {
-  int block, bps;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    block = g_block;
-    bps = g_blocks_per_sm;
-  }
-  switch (block) {
-    case 32: return launch_rollout<32>(a, ctrl, rc, npolicy, decim, cfg, rp, s, bps);
-    case 64: return launch_rollout<64>(a, ctrl, rc, npolicy, decim, cfg, rp, s, bps);
-    case 96: return launch_rollout<96>(a, ctrl, rc, npolicy, decim, cfg, rp, s, bps);
-    default: return launch_rollout<128>(a, ctrl, rc, npolicy, decim, cfg, rp, s, bps);
-  }
+int dispatch_step(const StateArgs& a, const float* ctrl, int nsub, const StepConfig& cfg, cudaStream_t s) {
+  RolloutParams rp{};
+  return dispatch(current_shape(), false, a, const_cast<float*>(ctrl), nullptr, 1, nsub, cfg, rp, s);
+}
+
+int dispatch_rollout(const StateArgs& a, float* ctrl, int* rc, int npolicy, int decim, const StepConfig& cfg,
+                     const RolloutParams& rp, cudaStream_t s) {
+  return dispatch(current_shape(), true, a, ctrl, rc, npolicy, decim, cfg, rp, s);
 }
 
 int check_state(int nenv, const void* qpos, const void* qvel, const void* anchor, const void* ctrl) {
@@ -470,28 +650,81 @@ void g1_cuda_reset_done(int nenv, float* qpos, float* qvel, float* anchor, const
   if (e != cudaSuccess) cuda_fail(e, "reset_done_kernel launch");
 }
 
-int g1b_set_launch(int block, int blocks_per_sm) {
+int g1b_set_launch(int mapping, int block, int blocks_per_sm) {
+  if (mapping != 0 && mapping != 1) return fail("mapping must be 0 (thread per env) or 1 (two threads per env)");
   if (block != 32 && block != 64 && block != 96 && block != 128) return fail("block must be 32, 64, 96 or 128");
   if (blocks_per_sm < 0) return fail("blocks_per_sm must be >= 0");
   std::lock_guard<std::mutex> lk(g_mu);
+  g_mapping = mapping;
   g_block = block;
   g_blocks_per_sm = blocks_per_sm;
   return 0;
 }
 
-int g1b_get_launch(int* block, int* blocks_per_sm) {
+int g1b_get_launch(int* mapping, int* block, int* blocks_per_sm) {
   std::lock_guard<std::mutex> lk(g_mu);
+  if (mapping) *mapping = g_mapping;
   if (block) *block = g_block;
   if (blocks_per_sm) *blocks_per_sm = g_blocks_per_sm;
   return 0;
 }
 
 int g1b_autotune(int nenv, int nsub, void* stream, float* best_ms) {
-  (void)nenv;
-  (void)nsub;
-  (void)stream;
-  (void)best_ms;
-  return fail("autotune: not built yet");
+  if (nenv <= 0 || nsub <= 0) return fail("autotune: nenv and nsub must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)nenv;
+  float* buf = nullptr;  // qpos, qvel, anchor, ctrl of a temporary state
+  const size_t floats = n * (kNQ + kNV + 2 * kNC + kNU);
+  cudaError_t e = cudaMalloc(&buf, floats * sizeof(float));
+  if (e != cudaSuccess) return cuda_fail(e, "autotune: cudaMalloc");
+  float *qpos = buf, *qvel = qpos + n * kNQ, *anchor = qvel + n * kNV, *ctrl = anchor + n * 2 * kNC;
+  StateArgs a{nenv, qpos, qvel, anchor, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  g1b_config c = default_cfg();
+  c.dt = 2e-3f;
+  const StepConfig cfg = to_cfg(&c);
+  RolloutParams rp{};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks[4] = {32, 64, 96, 128};
+  LaunchShape best{1, 128, 0};
+  float best_t = 1e30f;
+  int rc = 0;
+  for (int mapping = 0; mapping < 2 && rc == 0; ++mapping) {
+    for (int bi = 0; bi < 4 && rc == 0; ++bi) {
+      const LaunchShape L{mapping, blocks[bi], 0};
+      init_stand_kernel<<<(nenv + 127) / 128, 128, 0, st>>>(nenv, qpos, qvel, anchor, ctrl);
+      rc = dispatch(L, false, a, ctrl, nullptr, 1, 1, cfg, rp, st);  // warm-up
+      if (rc) break;
+      cudaEventRecord(e0, st);
+      rc = dispatch(L, false, a, ctrl, nullptr, 1, nsub, cfg, rp, st);
+      cudaEventRecord(e1, st);
+      if (rc) break;
+      e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        rc = cuda_fail(e, "autotune");
+        break;
+      }
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (t < best_t) {
+        best_t = t;
+        best = L;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_mapping = best.mapping;
+    g_block = best.block;
+    g_blocks_per_sm = best.bps;
+  }
+  if (best_ms) *best_ms = best_t;
+  return 0;
 }
 
 int g1b_ffma_peak(int iters, float* tflops, float* ms) {

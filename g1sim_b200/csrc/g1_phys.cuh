@@ -431,14 +431,23 @@ G1_HD SV bias_force(const AI& In, const V3& w, const V3& v, const V3& g) {
 }
 
 // ---------------------------------------------------------------- scratch
-// Per hinge h (body h + 1), slot h * 15 + k:
-//   0 q, 1 qd, 2 cos, 3 sin, 4-7 velocity-product term c (4 non-zeros),
-//   8-13 bias force pA (FK -> backward), then U / D (backward -> forward),
-//   14 u / D.
-// Slots kSlotPelvis.. +5: pelvis bias force.
-constexpr int kSlotsPerHinge = 15;
-constexpr int kSlotPelvis = kNJ * kSlotsPerHinge;
-constexpr int kNumSlots = kSlotPelvis + 6;
+// Per hinge h (body h + 1), slot h * 11 + k:
+//   0 q, 1 qd, 2 cos q, 3 sin q, 4-9 U / D (backward -> forward), 10 u / D.
+// Per chain c (0 left leg, 1 right leg, 2 waist, 3 left arm, 4 right arm):
+//   kSlotChain + 9 c: twist (6) and gravity (3) of the chain's last body
+//   (FK -> backward; the backward pass recovers the other bodies' twist and
+//   gravity by moving back up the chain).
+// Per foot f: kSlotFoot + 6 f: contact wrench on the foot body (body frame).
+// kSlotXchg..: exchanged between the two halves of a split step: the upper
+// body's projection into the pelvis (27: J 6, H 9, M 6, bias 6), the base
+// acceleration (6), the base state (13) and a reset flag (1).
+constexpr int kSlotsPerHinge = 11;
+constexpr int kSlotChain = kNJ * kSlotsPerHinge;
+constexpr int kSlotFoot = kSlotChain + 5 * 9;
+constexpr int kSlotXchg = kSlotFoot + 12;
+constexpr int kXUp = kSlotXchg, kXA0 = kSlotXchg + 27, kXBase = kSlotXchg + 33, kXReset = kSlotXchg + 46;
+constexpr int kNumSlotsSingle = kSlotXchg;  // one thread per env
+constexpr int kNumSlots = kSlotXchg + 47;   // two threads per env
 G1_CE int hslot(int body, int k) { return (body - 1) * kSlotsPerHinge + k; }
 
 // ----------------------------------------------------------- env data
@@ -487,15 +496,55 @@ G1_HD SV load_sv(Scr& scr, int s0) {
   return r;
 }
 template <class Scr>
-G1_HD SV load_bias(Scr& scr, int body) {
-  return load_sv(scr, body == 0 ? kSlotPelvis : hslot(body, 8));
+G1_HD void store_end(Scr& scr, int c, const FKNode& n) {
+  const int s0 = kSlotChain + 9 * c;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    scr.put(s0 + k, n.w.v[k]);
+    scr.put(s0 + 3 + k, n.v.v[k]);
+    scr.put(s0 + 6 + k, n.g.v[k]);
+  }
+}
+template <class Scr>
+G1_HD void load_end(Scr& scr, int c, V3& w, V3& v, V3& g) {
+  const int s0 = kSlotChain + 9 * c;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    w.v[k] = scr.get(s0 + k);
+    v.v[k] = scr.get(s0 + 3 + k);
+    g.v[k] = scr.get(s0 + 6 + k);
+  }
+}
+
+// chains: 0 left leg 1-6, 1 right leg 7-12, 2 waist 13-15, 3 left arm
+// 16-22, 4 right arm 23-29; legs and waist hang off the pelvis, arms off the
+// torso (15)
+G1_HD int chain_first(int c) { return c == 0 ? 1 : c == 1 ? 7 : c == 2 ? 13 : c == 3 ? 16 : 23; }
+G1_HD int chain_last(int c) { return c == 0 ? 6 : c == 1 ? 12 : c == 2 ? 15 : c == 3 ? 22 : 29; }
+
+G1_HD void sv_zero(SV& x) { x.a = x.l = mk3(0.f, 0.f, 0.f); }
+G1_HD void sv_acc(SV& x, const SV& y) {
+  x.a = add(x.a, y.a);
+  x.l = add(x.l, y.l);
+}
+
+// velocity-product term c = v x_m (qd S) = [qd (w x e_ax); qd (v x e_ax)]:
+// four non-zeros, angular i1, i2 then linear i1, i2
+template <int AX>
+G1_HD void vel_product(const V3& w, const V3& v, float qd, float* cv) {
+  constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
+  cv[0] = qd * w.v[i2];
+  cv[1] = -(qd * w.v[i1]);
+  cv[2] = qd * v.v[i2];
+  cv[3] = -(qd * v.v[i1]);
 }
 
 // ------------------------------------------------------------- FK pass
-// reference src/g1_core.h:29-54 (+ bias init :113-120 and the c term of :180)
+// reference src/g1_core.h:29-54: parent -> child twist and gravity; with
+// kWorld (legs) also the world pose in float-float, and the joint's sin/cos
+// from the extended-precision routine.
 template <int AX, bool kWorld, class Scr>
 G1_HD void fk_body(int i, FKNode& n, Scr& scr) {
-  constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
   const BodyC& b = body(i);
   const float q = scr.get(hslot(i, 0)), qd = scr.get(hslot(i, 1));
   float s, c;
@@ -534,16 +583,9 @@ G1_HD void fk_body(int i, FKNode& n, Scr& scr) {
   n.w = w;
   n.v = v;
   n.g = g;
-  // velocity-product term c = v x_m (qd S) = [qd (w x e_ax); qd (v x e_ax)]
-  scr.put(hslot(i, 4), qd * w.v[i2]);
-  scr.put(hslot(i, 5), -(qd * w.v[i1]));
-  scr.put(hslot(i, 6), qd * v.v[i2]);
-  scr.put(hslot(i, 7), -(qd * v.v[i1]));
-  store_sv(scr, hslot(i, 8), bias_force(body_inertia(b), w, v, g));
 }
 
-// FK of the serial chain first..last from the node of its parent; stores
-// each body's bias force.
+// FK of the serial chain first..last from the node of its parent.
 template <bool kWorld, class Scr>
 G1_HD void fk_chain(int first, int last, FKNode& n, Scr& scr) {
 #pragma unroll 1
@@ -559,10 +601,9 @@ G1_HD void fk_chain(int first, int last, FKNode& n, Scr& scr) {
 // --------------------------------------------------------------- contacts
 // Eight spheres, four on each foot (reference src/g1_core.h:123-153).  The
 // world wrench about the foot origin is accumulated and rotated to the body
-// frame once.
+// frame once; returns the wrench's contribution to the foot's bias force.
 template <int K0>
-G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const StepConfig& cfg, float mu,
-                         SV& pA_foot) {
+G1_HD SV foot_contacts(const FKNode& n, const EnvIO& io, bool last, const StepConfig& cfg, float mu) {
   float* anchor = io.anchor;
   const size_t sd = io.stride;
   const V3 ww = mv(n.R, n.w);  // world angular velocity
@@ -616,8 +657,10 @@ G1_HD void foot_contacts(const FKNode& n, const EnvIO& io, bool last, const Step
     }
     if (last && io.cf) io.cf[k * sd] = fn;
   }
-  pA_foot.a = sub(pA_foot.a, mtv(n.R, Tq));
-  pA_foot.l = sub(pA_foot.l, mtv(n.R, F));
+  SV r;
+  r.a = scl(-1.0f, mtv(n.R, Tq));
+  r.l = scl(-1.0f, mtv(n.R, F));
+  return r;
 }
 
 // --------------------------------------------------------- backward pass
@@ -670,11 +713,12 @@ G1_HD SV f_to_parent(const BodyC& b, const SV& f, float c, float s) {
 
 // One hinge of the backward pass with PD servo, soft limits and implicit
 // damping (reference src/g1_core.h:156-186).  IA, pA are body i's
-// articulated inertia and bias; the projected values are added into
-// (accI, accP), expressed in the parent's frame.
+// articulated inertia and bias, (w, v) its twist; the projected values are
+// added into (accI, accP), expressed in the parent's frame, and (w, v, g)
+// are moved to the parent: v_p = X (v_i - qd S), g_p = R g_i.
 template <int AX, class Scr>
-G1_HD void bwd_body(int i, const AI& IA, const SV& pA, AI& accI, SV& accP, const EnvIO& io,
-                    const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
+G1_HD void bwd_body(int i, const AI& IA, const SV& pA, V3& w, V3& v, V3& g, AI& accI, SV& accP,
+                    const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
   constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
   const BodyC& b = body(i);
   const int h = i - 1;
@@ -701,13 +745,8 @@ G1_HD void bwd_body(int i, const AI& IA, const SV& pA, AI& accI, SV& accP, const
   const float D = U.a.v[AX] + b.arm + cfg.dt * bd;
   const float u = t - b.damp * qd - pA.a.v[AX];
   const float invD = 1.0f / D;
-  SV cv;
-  cv.a.v[AX] = 0.0f;
-  cv.a.v[i1] = scr.get(hslot(i, 4));
-  cv.a.v[i2] = scr.get(hslot(i, 5));
-  cv.l.v[AX] = 0.0f;
-  cv.l.v[i1] = scr.get(hslot(i, 6));
-  cv.l.v[i2] = scr.get(hslot(i, 7));
+  float cv[4];
+  vel_product<AX>(w, v, qd, cv);
   // Ia = IA - U U^T / D
   SV W;
   W.a = scl(invD, U.a);
@@ -729,18 +768,25 @@ G1_HD void bwd_body(int i, const AI& IA, const SV& pA, AI& accI, SV& accP, const
   const float uD = u * invD;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    pa.a.v[a] = pA.a.v[a] + Ia.J.s[sidx(a, i1)] * cv.a.v[i1] + Ia.J.s[sidx(a, i2)] * cv.a.v[i2] +
-                Ia.H.m[3 * a + i1] * cv.l.v[i1] + Ia.H.m[3 * a + i2] * cv.l.v[i2] + uD * U.a.v[a];
-    pa.l.v[a] = pA.l.v[a] + Ia.H.m[3 * i1 + a] * cv.a.v[i1] + Ia.H.m[3 * i2 + a] * cv.a.v[i2] +
-                Ia.M.s[sidx(a, i1)] * cv.l.v[i1] + Ia.M.s[sidx(a, i2)] * cv.l.v[i2] + uD * U.l.v[a];
+    pa.a.v[a] = pA.a.v[a] + Ia.J.s[sidx(a, i1)] * cv[0] + Ia.J.s[sidx(a, i2)] * cv[1] +
+                Ia.H.m[3 * a + i1] * cv[2] + Ia.H.m[3 * a + i2] * cv[3] + uD * U.a.v[a];
+    pa.l.v[a] = pA.l.v[a] + Ia.H.m[3 * i1 + a] * cv[0] + Ia.H.m[3 * i2 + a] * cv[1] +
+                Ia.M.s[sidx(a, i1)] * cv[2] + Ia.M.s[sidx(a, i2)] * cv[3] + uD * U.l.v[a];
   }
-  // keep U / D and u / D for the forward pass (U / D in the bias slots)
-  store_sv(scr, hslot(i, 8), W);
-  scr.put(hslot(i, 14), uD);
+  // keep U / D and u / D for the forward pass
+  store_sv(scr, hslot(i, 4), W);
+  scr.put(hslot(i, 10), uD);
   ai_to_parent_add<AX>(b, accI, Ia, c, s);
   const SV fp = f_to_parent<AX>(b, pa, c, s);
   accP.a = add(accP.a, fp.a);
   accP.l = add(accP.l, fp.l);
+  // twist and gravity of the parent
+  V3 wm = w;
+  wm.v[AX] -= qd;
+  const V3 wp = rotT(b, rotA<AX>(wm, c, s));
+  v = add(rotT(b, rotA<AX>(v, c, s)), pcross(b, wp));
+  w = wp;
+  g = rotT(b, rotA<AX>(g, c, s));
 }
 
 G1_HD void ai_zero(AI& A) {
@@ -759,34 +805,35 @@ G1_HD void ai_add(AI& A, const AI& B) {
   for (int k = 0; k < 9; ++k) A.H.m[k] += B.H.m[k];
 }
 
-// Backward pass over the serial chain first..last, starting from the
-// articulated inertia / bias (IA, pA) of its last body; adds the chain's
-// projection into its parent's accumulators (accI, accP).
+// Backward pass over the serial chain first..last.  (IA, pA) are the
+// articulated inertia and bias of its last body and (w, v, g) that body's
+// twist and gravity; the chain's projection into its parent is returned in
+// (outI, outP).  Each body's rigid bias force is computed here from the
+// recovered twist (reference src/g1_core.h:113-120).
 template <class Scr>
-G1_HD void bwd_chain(int first, int last, AI IA, SV pA, AI& accI, SV& accP, const EnvIO& io,
-                     const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
+G1_HD void bwd_chain(int first, int last, AI IA, SV pA, V3 w, V3 v, V3 g, AI& outI, SV& outP,
+                     const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr) {
 #pragma unroll 1
   for (int i = last; i >= first; --i) {
     AI IAp;
     SV pAp;
     if (i > first) {
       IAp = body_inertia(body(i - 1));
-      pAp = load_bias(scr, i - 1);
     } else {
       ai_zero(IAp);
-      pAp.a = pAp.l = mk3(0.f, 0.f, 0.f);
     }
+    sv_zero(pAp);
     switch (body(i).axis) {
-      case 0: bwd_body<0>(i, IA, pA, IAp, pAp, io, ep, cfg, scr); break;
-      case 1: bwd_body<1>(i, IA, pA, IAp, pAp, io, ep, cfg, scr); break;
-      default: bwd_body<2>(i, IA, pA, IAp, pAp, io, ep, cfg, scr); break;
+      case 0: bwd_body<0>(i, IA, pA, w, v, g, IAp, pAp, io, ep, cfg, scr); break;
+      case 1: bwd_body<1>(i, IA, pA, w, v, g, IAp, pAp, io, ep, cfg, scr); break;
+      default: bwd_body<2>(i, IA, pA, w, v, g, IAp, pAp, io, ep, cfg, scr); break;
     }
+    if (i > first) sv_acc(pAp, bias_force(body_inertia(body(i - 1)), w, v, g));
     IA = IAp;
     pA = pAp;
   }
-  ai_add(accI, IA);
-  accP.a = add(accP.a, pA.a);
-  accP.l = add(accP.l, pA.l);
+  outI = IA;
+  outP = pA;
 }
 
 // ---------------------------------------------------------- base solve
@@ -837,41 +884,51 @@ G1_HD SV base_solve(const AI& A, const SV& pA) {
 }
 
 // --------------------------------------------------------- forward pass
+// The twist is carried down the chain again (v_i = X^-1 v_p + qd S, with the
+// rate before this substep's update) for the velocity-product term;
 // a_i = X^-1 a_p + c_i ; qdd = u/D - (U/D).a_i ; a_i += qdd S  (reference
 // src/g1_core.h:190-201), fused with the hinge's semi-implicit Euler update
 // (reference src/g1_core.h:214,221).
 template <int AX, class Scr>
-G1_HD void fwd_body(int i, SV& a, float dt, Scr& scr) {
+G1_HD void fwd_body(int i, SV& a, V3& w, V3& v, float dt, Scr& scr) {
   constexpr int i1 = (AX + 1) % 3, i2 = (AX + 2) % 3;
   const BodyC& b = body(i);
   const float c = scr.get(hslot(i, 2)), s = scr.get(hslot(i, 3));
+  const float qd0 = scr.get(hslot(i, 1));
+  // twist of body i (as in the FK pass)
+  const V3 tv = sub(v, pcross(b, w));
+  w = rotAT<AX>(rotTT(b, w), c, s);
+  v = rotAT<AX>(rotTT(b, tv), c, s);
+  w.v[AX] += qd0;
+  float cv[4];
+  vel_product<AX>(w, v, qd0, cv);
   const V3 t = sub(a.l, pcross(b, a.a));
   SV an;
   an.a = rotAT<AX>(rotTT(b, a.a), c, s);
   an.l = rotAT<AX>(rotTT(b, t), c, s);
-  an.a.v[i1] += scr.get(hslot(i, 4));
-  an.a.v[i2] += scr.get(hslot(i, 5));
-  an.l.v[i1] += scr.get(hslot(i, 6));
-  an.l.v[i2] += scr.get(hslot(i, 7));
-  const SV W = load_sv(scr, hslot(i, 8));  // U / D
-  const float uD = scr.get(hslot(i, 14));   // u / D
+  an.a.v[i1] += cv[0];
+  an.a.v[i2] += cv[1];
+  an.l.v[i1] += cv[2];
+  an.l.v[i2] += cv[3];
+  const SV W = load_sv(scr, hslot(i, 4));  // U / D
+  const float uD = scr.get(hslot(i, 10));  // u / D
   const float qdd = uD - (W.a.v[0] * an.a.v[0] + W.a.v[1] * an.a.v[1] + W.a.v[2] * an.a.v[2] +
                           W.l.v[0] * an.l.v[0] + W.l.v[1] * an.l.v[1] + W.l.v[2] * an.l.v[2]);
   an.a.v[AX] += qdd;
   a = an;
-  const float qd = scr.get(hslot(i, 1)) + dt * qdd;
+  const float qd = qd0 + dt * qdd;
   scr.put(hslot(i, 1), qd);
   scr.put(hslot(i, 0), scr.get(hslot(i, 0)) + dt * qd);
 }
 
 template <class Scr>
-G1_HD void fwd_chain(int first, int last, SV& a, float dt, Scr& scr) {
+G1_HD void fwd_chain(int first, int last, SV& a, V3& w, V3& v, float dt, Scr& scr) {
 #pragma unroll 1
   for (int i = first; i <= last; ++i) {
     switch (body(i).axis) {
-      case 0: fwd_body<0>(i, a, dt, scr); break;
-      case 1: fwd_body<1>(i, a, dt, scr); break;
-      default: fwd_body<2>(i, a, dt, scr); break;
+      case 0: fwd_body<0>(i, a, w, v, dt, scr); break;
+      case 1: fwd_body<1>(i, a, w, v, dt, scr); break;
+      default: fwd_body<2>(i, a, w, v, dt, scr); break;
     }
   }
 }
@@ -890,7 +947,6 @@ G1_HD void quat_normalized(const float* q, float* r) {
   for (int k = 0; k < 4; ++k) r[k] = q[k] * inv;
 }
 
-// ----------------------------------------------------------------- step
 // Base frame quantities from the state: rotation, body twist, body gravity.
 G1_HD void base_node(const EnvState& st, const StepConfig& cfg, FKNode& base) {
   float qn[4];
@@ -939,151 +995,243 @@ G1_HD void foot_outputs(const FKNode& n, const EnvIO& io, int o) {
   }
 }
 
-// Chains in the order each phase visits them.  FK / forward: legs, waist,
-// arms (the arms need the torso); backward: arms, waist, legs (the waist
-// needs both arms).  first, last body; the parent is the pelvis for legs and
-// waist, the torso for arms.
-G1_HD int chain_first(int c) { return c == 0 ? 1 : c == 1 ? 7 : c == 2 ? 13 : c == 3 ? 16 : 23; }
-G1_HD int chain_last(int c) { return c == 0 ? 6 : c == 1 ? 12 : c == 2 ? 15 : c == 3 ? 22 : 29; }
-
-G1_HD void sv_zero(SV& x) { x.a = x.l = mk3(0.f, 0.f, 0.f); }
-G1_HD void sv_acc(SV& x, const SV& y) {
-  x.a = add(x.a, y.a);
-  x.l = add(x.l, y.l);
+// ============================================================ exchange
+template <class Scr>
+G1_HD void store_ai(Scr& scr, int s0, const AI& A, const SV& p) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) scr.put(s0 + k, A.J.s[k]);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) scr.put(s0 + 6 + k, A.H.m[k]);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) scr.put(s0 + 15 + k, A.M.s[k]);
+  store_sv(scr, s0 + 21, p);
+}
+template <class Scr>
+G1_HD void load_ai(Scr& scr, int s0, AI& A, SV& p) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) A.J.s[k] = scr.get(s0 + k);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) A.H.m[k] = scr.get(s0 + 6 + k);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) A.M.s[k] = scr.get(s0 + 15 + k);
+  p = load_sv(scr, s0 + 21);
+}
+template <class Scr>
+G1_HD void store_base(Scr& scr, const EnvState& st) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) scr.put(kXBase + k, st.pos[k]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) scr.put(kXBase + 3 + k, st.quat[k]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) scr.put(kXBase + 7 + k, st.vw[k]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) scr.put(kXBase + 10 + k, st.wb[k]);
+}
+template <class Scr>
+G1_HD void load_base(Scr& scr, EnvState& st) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.pos[k] = scr.get(kXBase + k);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) st.quat[k] = scr.get(kXBase + 3 + k);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.vw[k] = scr.get(kXBase + 7 + k);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.wb[k] = scr.get(kXBase + 10 + k);
 }
 
-// One substep: FK -> contacts -> PD + ABA -> integrate (reference
-// src/g1_core.h:225-232).  Joint angles / rates are read from and written
-// back to the scratch.  With last_sub set, the foot kinematics of this
-// substep's FK (before integration) and the contact normal forces are
-// written to io's outputs.  Each phase is ONE loop over the chains so that
-// every hinge routine is instantiated once (per axis).
+// ================================================================= phases
+// The substep split in the phases of the two halves of the tree: the lower
+// body (pelvis, legs, contacts, base) and the upper body (waist, arms).  One
+// thread runs all of them in order (step); the split kernel runs the lower
+// phases on one thread and the upper phases on another, exchanging the upper
+// body's projection into the pelvis, the base acceleration and the base
+// state through the scratch.
+
+// FK of the legs in extended precision, contacts; stores chain ends, foot
+// wrenches and (last substep) the foot outputs.
+template <class Scr>
+G1_HD void fk_lower(const EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
+                    bool last_sub) {
+  FKNode base;
+  base_node(st, cfg, base);
+  base_pose_ff(st, base);
+#pragma unroll 1
+  for (int c = 0; c < 2; ++c) {
+    FKNode n = base;
+    fk_chain<true>(chain_first(c), chain_last(c), n, scr);
+    const SV wr = c == 0 ? foot_contacts<0>(n, io, last_sub, cfg, ep.mu) : foot_contacts<4>(n, io, last_sub, cfg, ep.mu);
+    store_sv(scr, kSlotFoot + 6 * c, wr);
+    store_end(scr, c, n);
+    if (last_sub) foot_outputs(n, io, c == 0 ? 0 : 3);
+  }
+}
+
+// FK of the waist and the arms; stores chain ends.
+template <class Scr>
+G1_HD void fk_upper(const EnvState& st, const StepConfig& cfg, Scr& scr) {
+  FKNode n;
+  base_node(st, cfg, n);
+  fk_chain<false>(13, 15, n, scr);
+  store_end(scr, 2, n);
+  const FKNode torso = n;
+#pragma unroll 1
+  for (int c = 3; c < 5; ++c) {
+    n = torso;
+    fk_chain<false>(chain_first(c), chain_last(c), n, scr);
+    store_end(scr, c, n);
+  }
+}
+
+// Backward pass of the arms into the torso and of the waist: the upper
+// body's projection into the pelvis frame.
+template <class Scr>
+G1_HD void bwd_upper(const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr, AI& outI, SV& outP) {
+  V3 w15, v15, g15;
+  load_end(scr, 2, w15, v15, g15);
+  AI acc15 = body_inertia(body(15));
+  SV accP15 = bias_force(acc15, w15, v15, g15);
+#pragma unroll 1
+  for (int c = 3; c < 5; ++c) {
+    V3 w, v, g;
+    load_end(scr, c, w, v, g);
+    const int last = chain_last(c);
+    const AI IA = body_inertia(body(last));
+    AI ci;
+    SV cp;
+    bwd_chain(chain_first(c), last, IA, bias_force(IA, w, v, g), w, v, g, ci, cp, io, ep, cfg, scr);
+    ai_add(acc15, ci);
+    sv_acc(accP15, cp);
+  }
+  bwd_chain(13, 15, acc15, accP15, w15, v15, g15, outI, outP, io, ep, cfg, scr);
+}
+
+// Backward pass of the legs into the pelvis accumulators (pelvis inertia and
+// bias included).
+template <class Scr>
+G1_HD void bwd_lower(const EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
+                     AI& acc0, SV& accP0) {
+  {
+    FKNode base;
+    base_node(st, cfg, base);
+    acc0 = pelvis_inertia(ep.dmass);
+    accP0 = bias_force(acc0, base.w, base.v, base.g);
+  }
+#pragma unroll 1
+  for (int c = 0; c < 2; ++c) {
+    V3 w, v, g;
+    load_end(scr, c, w, v, g);
+    const int last = chain_last(c);
+    const AI IA = body_inertia(body(last));
+    SV pA = bias_force(IA, w, v, g);
+    sv_acc(pA, load_sv(scr, kSlotFoot + 6 * c));
+    AI ci;
+    SV cp;
+    bwd_chain(chain_first(c), last, IA, pA, w, v, g, ci, cp, io, ep, cfg, scr);
+    ai_add(acc0, ci);
+    sv_acc(accP0, cp);
+  }
+}
+
+// Forward pass of the legs, then the base integration (semi-implicit Euler;
+// base qacc in MuJoCo's free-joint convention, world linear incl. w x v and
+// body angular, reference src/g1_core.h:203-206,215-220).
+template <class Scr>
+G1_HD void fwd_lower_and_base(EnvState& st, const SV& a0, const StepConfig& cfg, Scr& scr) {
+  const float dt = cfg.dt;
+  FKNode base;
+  base_node(st, cfg, base);
+#pragma unroll 1
+  for (int c = 0; c < 2; ++c) {
+    SV a = a0;
+    V3 w = base.w, v = base.v;
+    fwd_chain(chain_first(c), chain_last(c), a, w, v, dt, scr);
+  }
+  const V3 al = mv(base.R, add(a0.l, crs(base.w, base.v)));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.vw[k] += dt * al.v[k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
+  // q <- q (x) exp(w dt / 2), renormalised (reference src/spatial.h:73-79)
+  const float wx = st.wb[0], wy = st.wb[1], wz = st.wb[2];
+  const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
+  const float angle = wn * dt;
+  if (angle >= 1e-12f) {
+    float sh, ch;
+    sincosf(0.5f * angle, &sh, &ch);
+    const float k = sh / wn;
+    const float dq[4] = {ch, k * wx, k * wy, k * wz};
+    const float* q = st.quat;
+    float r[4];
+    r[0] = q[0] * dq[0] - q[1] * dq[1] - q[2] * dq[2] - q[3] * dq[3];
+    r[1] = q[0] * dq[1] + q[1] * dq[0] + q[2] * dq[3] - q[3] * dq[2];
+    r[2] = q[0] * dq[2] - q[1] * dq[3] + q[2] * dq[0] + q[3] * dq[1];
+    r[3] = q[0] * dq[3] + q[1] * dq[2] - q[2] * dq[1] + q[3] * dq[0];
+    quat_normalized(r, st.quat);
+  }
+}
+
+// Forward pass of the waist and the arms (the base state is not touched).
+template <class Scr>
+G1_HD void fwd_upper(const EnvState& st, const SV& a0, const StepConfig& cfg, Scr& scr) {
+  const float dt = cfg.dt;
+  FKNode base;
+  base_node(st, cfg, base);
+  SV a = a0;
+  V3 w = base.w, v = base.v;
+  fwd_chain(13, 15, a, w, v, dt, scr);
+  const SV a15 = a;
+  const V3 w15 = w, v15 = v;
+#pragma unroll 1
+  for (int c = 3; c < 5; ++c) {
+    a = a15;
+    w = w15;
+    v = v15;
+    fwd_chain(chain_first(c), chain_last(c), a, w, v, dt, scr);
+  }
+}
+
+// One substep on one thread: FK -> contacts -> PD + ABA -> integrate
+// (reference src/g1_core.h:225-232).  Joint angles / rates are read from and
+// written back to the scratch.  With last_sub set, the foot kinematics of
+// this substep's FK (before integration) and the contact normal forces are
+// written to io's outputs.
 template <class Scr>
 G1_HD void step(EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
                 bool last_sub) {
-  // ---- FK + bias forces + contacts: legs (world pose), waist, arms
-  {
-    FKNode base;
-    base_node(st, cfg, base);
-    base_pose_ff(st, base);
-    store_sv(scr, kSlotPelvis, bias_force(pelvis_inertia(ep.dmass), base.w, base.v, base.g));
-    FKNode torso = base;
-#pragma unroll 1
-    for (int c = 0; c < 5; ++c) {
-      FKNode n = c < 3 ? base : torso;
-      const int first = chain_first(c), last = chain_last(c);
-      if (c < 2) {
-        fk_chain<true>(first, last, n, scr);
-        SV pA = load_bias(scr, last);
-        if (c == 0)
-          foot_contacts<0>(n, io, last_sub, cfg, ep.mu, pA);
-        else
-          foot_contacts<4>(n, io, last_sub, cfg, ep.mu, pA);
-        store_sv(scr, hslot(last, 8), pA);
-        if (last_sub) foot_outputs(n, io, c == 0 ? 0 : 3);
-      } else {
-        fk_chain<false>(first, last, n, scr);
-        if (c == 2) torso = n;
-      }
-    }
-  }
-  // ---- backward: arms into the torso, the waist (from the torso) and the
-  // legs into the pelvis
-  AI acc0 = pelvis_inertia(ep.dmass);
-  SV accP0 = load_bias(scr, 0);
-  {
-    AI acc15 = body_inertia(body(15));
-    SV accP15 = load_bias(scr, 15);
-#pragma unroll 1
-    for (int k = 0; k < 5; ++k) {
-      const int c = k == 0 ? 3 : k == 1 ? 4 : k == 2 ? 2 : k == 3 ? 0 : 1;
-      const int first = chain_first(c), last = chain_last(c);
-      AI IA;
-      SV pA;
-      if (c == 2) {
-        IA = acc15;
-        pA = accP15;
-      } else {
-        IA = body_inertia(body(last));
-        pA = load_bias(scr, last);
-      }
-      AI contrib;
-      SV contribP;
-      ai_zero(contrib);
-      sv_zero(contribP);
-      bwd_chain(first, last, IA, pA, contrib, contribP, io, ep, cfg, scr);
-      if (c >= 3) {
-        ai_add(acc15, contrib);
-        sv_acc(accP15, contribP);
-      } else {
-        ai_add(acc0, contrib);
-        sv_acc(accP0, contribP);
-      }
-    }
-  }
-  // ---- base acceleration
+  fk_lower(st, io, ep, cfg, scr, last_sub);
+  fk_upper(st, cfg, scr);
+  AI up;
+  SV upP;
+  bwd_upper(io, ep, cfg, scr, up, upP);
+  AI acc0;
+  SV accP0;
+  bwd_lower(st, io, ep, cfg, scr, acc0, accP0);
+  ai_add(acc0, up);
+  sv_acc(accP0, upP);
   const SV a0 = base_solve(acc0, accP0);
-  const float dt = cfg.dt;
-  // base velocity: MuJoCo free-joint qacc (world linear incl. w x v, body
-  // angular) from the pre-integration base frame
-  {
-    FKNode base;
-    base_node(st, cfg, base);
-    const V3 al = mv(base.R, add(a0.l, crs(base.w, base.v)));
-#pragma unroll
-    for (int k = 0; k < 3; ++k) st.vw[k] += dt * al.v[k];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
-  }
-  // ---- forward pass, fused with the hinge integration: legs, waist, arms
-  {
-    SV a15 = a0;
-#pragma unroll 1
-    for (int c = 0; c < 5; ++c) {
-      SV a = c < 3 ? a0 : a15;
-      fwd_chain(chain_first(c), chain_last(c), a, dt, scr);
-      if (c == 2) a15 = a;
-    }
-  }
-  // ---- base position and orientation (semi-implicit Euler)
-#pragma unroll
-  for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
-  {
-    // q <- q (x) exp(w dt / 2), renormalised (reference src/spatial.h:73-79)
-    const float wx = st.wb[0], wy = st.wb[1], wz = st.wb[2];
-    const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
-    const float angle = wn * dt;
-    if (angle >= 1e-12f) {
-      float sh, ch;
-      sincosf(0.5f * angle, &sh, &ch);
-      const float k = sh / wn;
-      const float dq[4] = {ch, k * wx, k * wy, k * wz};
-      const float* a = st.quat;
-      float r[4];
-      r[0] = a[0] * dq[0] - a[1] * dq[1] - a[2] * dq[2] - a[3] * dq[3];
-      r[1] = a[0] * dq[1] + a[1] * dq[0] + a[2] * dq[3] - a[3] * dq[2];
-      r[2] = a[0] * dq[2] - a[1] * dq[3] + a[2] * dq[0] + a[3] * dq[1];
-      r[3] = a[0] * dq[3] + a[1] * dq[2] - a[2] * dq[1] + a[3] * dq[0];
-      quat_normalized(r, st.quat);
-    }
-  }
+  fwd_upper(st, a0, cfg, scr);
+  fwd_lower_and_base(st, a0, cfg, scr);
 }
 
-// Joint angles / rates between the SoA state arrays and the scratch.
+// Joint angles / rates between the SoA state arrays and the scratch, for the
+// hinges of bodies first..last.
 template <class Scr>
-G1_HD void load_joints(const float* qpos, const float* qvel, size_t stride, Scr& scr) {
+G1_HD void load_joints(const float* qpos, const float* qvel, size_t stride, Scr& scr, int first = 1,
+                       int last = kNJ) {
 #pragma unroll 1
-  for (int h = 0; h < kNJ; ++h) {
-    scr.put(hslot(h + 1, 0), qpos[(7 + h) * stride]);
-    scr.put(hslot(h + 1, 1), qvel[(6 + h) * stride]);
+  for (int i = first; i <= last; ++i) {
+    scr.put(hslot(i, 0), qpos[(6 + i) * stride]);
+    scr.put(hslot(i, 1), qvel[(5 + i) * stride]);
   }
 }
 template <class Scr>
-G1_HD void store_joints(float* qpos, float* qvel, size_t stride, Scr& scr) {
+G1_HD void store_joints(float* qpos, float* qvel, size_t stride, Scr& scr, int first = 1, int last = kNJ) {
 #pragma unroll 1
-  for (int h = 0; h < kNJ; ++h) {
-    qpos[(7 + h) * stride] = scr.get(hslot(h + 1, 0));
-    qvel[(6 + h) * stride] = scr.get(hslot(h + 1, 1));
+  for (int i = first; i <= last; ++i) {
+    qpos[(6 + i) * stride] = scr.get(hslot(i, 0));
+    qvel[(5 + i) * stride] = scr.get(hslot(i, 1));
   }
 }
 

@@ -81,12 +81,15 @@ int g1b_rollout(int nenv, int npolicy, int decim, const g1b_config* cfg,
                 const float* mu, const float* dmass, int* reset_count, float* foot_pos,
                 float* foot_vel, float* contact_forces, void* stream);
 
-/* Launch shape of the step kernels: threads per block (32, 64, 96 or 128)
- * and resident blocks per SM used to size the persistent grid (0 = all
- * that fit).  g1b_autotune times the candidates on the current device for
- * a workload of nenv envs and keeps the fastest; g1b_get_launch reports it. */
-int g1b_set_launch(int block, int blocks_per_sm);
-int g1b_get_launch(int* block, int* blocks_per_sm);
+/* Launch shape of the step kernels.  mapping 0: one thread per env, block =
+ * envs (= threads) per block; mapping 1 (default): two threads per env, the
+ * lower body (pelvis, legs, contacts, base) and the upper body (waist, arms)
+ * on separate warps, block = envs per block (2 * block threads).  block is
+ * 32, 64, 96 or 128; blocks_per_sm caps the persistent grid (0 = all that
+ * fit).  g1b_autotune times the candidates on the current device for a
+ * workload of nenv envs and keeps the fastest; g1b_get_launch reports it. */
+int g1b_set_launch(int mapping, int block, int blocks_per_sm);
+int g1b_get_launch(int* mapping, int* block, int* blocks_per_sm);
 int g1b_autotune(int nenv, int nsub, void* stream, float* best_ms);
 
 /* FP32 FMA throughput microbenchmark (the FP32-pipe roofline denominator):

@@ -30,6 +30,18 @@ pytestmark = pytest.mark.gpu
 
 DEV = torch.device("cuda", 0)
 
+# launch shapes: (mapping, envs per block); mapping 0 = one thread per env,
+# 1 = two threads per env (lower / upper body on separate warps)
+SHAPES = [(0, 128), (1, 128), (1, 32)]
+
+
+@pytest.fixture(params=SHAPES, ids=lambda s: f"map{s[0]}-b{s[1]}")
+def shape(request):
+    prev = _lib.get_launch()
+    _lib.set_launch(*request.param)
+    yield request.param
+    _lib.set_launch(*prev)
+
 
 def dev(a, dtype=torch.float32):
     return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
@@ -89,7 +101,7 @@ def _per_step_errors(oracle, nenv, steps, dt=2e-3, mu=None, dmass=None, seed=0):
             np.where(keep, np.array(ea), 0.0), np.array(ef), near)
 
 
-def test_drop_test_per_step_parity(oracle):
+def test_drop_test_per_step_parity(oracle, shape):
     """1,024-env drop test at dt = 2 ms, 250 steps, every step checked."""
     eq, ev, ea, ef, near = _per_step_errors(oracle, 1024, 250)
     print(f"qpos max {eq.max():.2e} | qvel median {np.median(ev):.2e} p99 {np.percentile(ev, 99):.2e} "
@@ -103,7 +115,7 @@ def test_drop_test_per_step_parity(oracle):
     assert ef.max() < 1e-4
 
 
-def test_randomized_params_per_step_parity(oracle):
+def test_randomized_params_per_step_parity(oracle, shape):
     rng = np.random.default_rng(5)
     n = 256
     mu = rng.uniform(0.4, 1.0, n).astype(np.float32).astype(np.float64)
@@ -139,7 +151,7 @@ def test_reference_abi_step_dt_1ms(oracle, golden_abi):
     assert np.abs(host(cf) - ocf).max() < 0.5
 
 
-def test_rollout_targets_bit_exact_and_parity(oracle):
+def test_rollout_targets_bit_exact_and_parity(oracle, shape):
     """Decimated randomised rollout: redrawn targets equal the oracle's bit for
     bit; each policy step (10 substeps at 2 ms) matches the oracle from the
     same state; resets happen where the oracle resets."""
@@ -174,7 +186,7 @@ def test_rollout_targets_bit_exact_and_parity(oracle):
     assert resets_gpu > 0
 
 
-def test_rollout_is_deterministic_and_composes():
+def test_rollout_is_deterministic_and_composes(shape):
     """rollout(npolicy=4) == 4 x rollout(npolicy=1, step0=k), bit for bit."""
     n = 300
     w = workloads.randomized(nenv=n, seed=2)
@@ -190,13 +202,44 @@ def test_rollout_is_deterministic_and_composes():
 
 
 @pytest.mark.parametrize("n", [1, 31, 33, 129, 1000])
-def test_ragged_env_counts(oracle, n):
+def test_ragged_env_counts(oracle, n, shape):
     w = workloads.drop_test(nenv=n, seed=11)
     qp, qv, an, ct = (dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
     G.step(qp, qv, an, ct, 3, config=_lib.default_config(dt=2e-3))
     q64, v64, a64 = (w[k].copy() for k in ("qpos", "qvel", "anchor"))
     oracle.step_soa(3, oracle.config(dt=2e-3), q64, v64, a64, w["ctrl"], outputs=False)
     assert relerr(host(qp), q64).max() < 1e-5
+
+
+def test_mappings_agree():
+    """One thread per env and two threads per env compute the same step."""
+    w = workloads.randomized(nenv=1000, seed=4)
+    out = []
+    prev = _lib.get_launch()
+    try:
+        for shp in SHAPES:
+            _lib.set_launch(*shp)
+            t = [dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl")]
+            G.rollout(*t, 3, 10, seed=9, mu=dev(w["mu"]), dmass=dev(w["dmass"]))
+            torch.cuda.synchronize()
+            out.append([host(x) for x in t])
+    finally:
+        _lib.set_launch(*prev)
+    for other in out[1:]:
+        for x, y in zip(out[0], other):
+            ok = (x < 1e29) & (y < 1e29)
+            assert relerr(x[ok], y[ok]).max(initial=0.0) < 1e-4
+
+
+def test_autotune_picks_a_valid_shape():
+    prev = _lib.get_launch()
+    try:
+        mapping, block, bps, ms = _lib.autotune(8192, 10)
+        assert mapping in (0, 1) and block in (32, 64, 96, 128) and ms > 0
+    finally:
+        _lib.set_launch(*prev)
+    with pytest.raises(RuntimeError):
+        _lib.set_launch(2, 128)
 
 
 def test_invalid_arguments_are_reported_not_launched():
