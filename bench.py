@@ -270,6 +270,9 @@ def ours(args, world, rank, local):
     _lib.check(L.g1b_ffma_peak(20000, C.byref(ffma_tf), C.byref(ffma_ms)), "g1b_ffma_peak")
     peak_tf = float(ffma_tf.value)
     hbm_gbs = BYTES_PER_ENV_LAUNCH * n / (launch_ms * 1e-3) / 1e9
+    mapping, block, _ = _lib.get_launch()
+    kernel_name = (f"split_kernel<{block}, rollout> (2 threads per env), 1 policy step" if mapping == 1
+                   else f"rollout_kernel<{block}> (1 thread per env), 1 policy step")
 
     # ---- single-launch (fully persistent) variant, reported alongside
     with torch.cuda.stream(stream):
@@ -328,7 +331,7 @@ def ours(args, world, rank, local):
             "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                          "frac": achieved_tf / peak_tf if peak_tf > 0 else None, "traffic": None,
                          "peak_source": "measured FFMA microbenchmark (g1b_ffma_peak), this run",
-                         "flops_per_env_step": FLOPS_PER_ENV_STEP, "kernel": "rollout_kernel, 1 policy step",
+                         "flops_per_env_step": FLOPS_PER_ENV_STEP, "kernel": kernel_name,
                          "kernel_ms": launch_ms, "hbm_gbs": hbm_gbs},
             "e2e": {"value": e2e_value, "unit": "env-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,

@@ -602,8 +602,7 @@ G1_HD void fk_chain(int first, int last, FKNode& n, Scr& scr) {
 // Eight spheres, four on each foot (reference src/g1_core.h:123-153).  The
 // world wrench about the foot origin is accumulated and rotated to the body
 // frame once; returns the wrench's contribution to the foot's bias force.
-template <int K0>
-G1_HD SV foot_contacts(const FKNode& n, const EnvIO& io, bool last, const StepConfig& cfg, float mu) {
+G1_HD SV foot_contacts(int K0, const FKNode& n, const EnvIO& io, bool last, const StepConfig& cfg, float mu) {
   float* anchor = io.anchor;
   const size_t sd = io.stride;
   const V3 ww = mv(n.R, n.w);  // world angular velocity
@@ -612,7 +611,7 @@ G1_HD SV foot_contacts(const FKNode& n, const EnvIO& io, bool last, const StepCo
   const float radius = (float)g1m_contact_radius;
   const float inv_kt = 1.0f / cfg.contact_kt;
   const ModelC& M = model();
-#pragma unroll
+#pragma unroll 1
   for (int k = K0; k < K0 + 4; ++k) {
     const V3 r = mk3(M.contact_pos[3 * k], M.contact_pos[3 * k + 1], M.contact_pos[3 * k + 2]);
     const V3 rw = mv(n.R, r);
@@ -1059,7 +1058,7 @@ G1_HD void fk_lower(const EnvState& st, const EnvIO& io, const EnvParams& ep, co
   for (int c = 0; c < 2; ++c) {
     FKNode n = base;
     fk_chain<true>(chain_first(c), chain_last(c), n, scr);
-    const SV wr = c == 0 ? foot_contacts<0>(n, io, last_sub, cfg, ep.mu) : foot_contacts<4>(n, io, last_sub, cfg, ep.mu);
+    const SV wr = foot_contacts(4 * c, n, io, last_sub, cfg, ep.mu);
     store_sv(scr, kSlotFoot + 6 * c, wr);
     store_end(scr, c, n);
     if (last_sub) foot_outputs(n, io, c == 0 ? 0 : 3);
