@@ -25,6 +25,35 @@ class RolloutParams(C.Structure):
                 ("redraw", C.c_int)]
 
 
+class Policy(C.Structure):
+    """g1b_policy: packed actor-critic (device pointers)."""
+    _fields_ = [("weights", C.c_void_p), ("bias", C.c_void_p), ("log_std", C.c_void_p),
+                ("obs_mean", C.c_void_p), ("obs_var", C.c_void_p)]
+
+
+class TaskState(C.Structure):
+    """g1b_task_state: per-env task state (device pointers, SoA)."""
+    _fields_ = [("commands", C.c_void_p), ("prev_action", C.c_void_p), ("cmd_timer", C.c_void_p),
+                ("ep_len", C.c_void_p), ("push_timer", C.c_void_p)]
+
+
+class TaskParams(C.Structure):
+    """g1b_task_params."""
+    _fields_ = [("seed", C.c_uint), ("step0", C.c_int), ("cmd_lo", C.c_float * 3), ("cmd_hi", C.c_float * 3),
+                ("cmd_steps_lo", C.c_int), ("cmd_steps_hi", C.c_int), ("push_steps_lo", C.c_int),
+                ("push_steps_hi", C.c_int), ("push_vel", C.c_float * 6), ("max_episode", C.c_int),
+                ("tilt_limit", C.c_float), ("reset_seed", C.c_uint), ("reset_noise", C.c_float),
+                ("reset_drop", C.c_float), ("flags", C.c_int)]
+
+
+class RolloutOut(C.Structure):
+    """g1b_rollout_out: per-step outputs (device pointers, each nullable)."""
+    _fields_ = [(n, C.c_void_p) for n in ("obs", "actions", "mean", "logp", "value", "reward", "done", "reset",
+                                         "last_obs", "last_value")]
+
+
+SAMPLE, PUSH, RESET, COMMANDS = 1, 2, 4, 8
+
 _vp = C.c_void_p
 
 
@@ -50,6 +79,12 @@ def lib():
     L.g1b_get_launch.argtypes = [C.POINTER(C.c_int)] * 3
     L.g1b_autotune.argtypes = [C.c_int, C.c_int, _vp, C.POINTER(C.c_float)]
     L.g1b_ffma_peak.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.g1b_policy_default_params.argtypes = [C.POINTER(TaskParams)]
+    L.g1b_policy_sizes.argtypes = [C.POINTER(C.c_int)] * 4
+    L.g1b_policy_rollout.argtypes = ([C.c_int, C.c_int, C.c_int, C.POINTER(Config), C.POINTER(TaskParams),
+                                      C.POINTER(Policy)] + [_vp] * 6 +
+                                     [C.POINTER(TaskState), C.POINTER(RolloutOut)] + [_vp] * 4)
+    L.g1b_policy_status.argtypes = [C.POINTER(C.c_int)]
     _lib = L
     return L
 
@@ -89,3 +124,22 @@ def get_launch():
 
 def last_error():
     return lib().g1b_last_error().decode(errors="replace")
+
+
+def policy_default_params():
+    p = TaskParams()
+    check(lib().g1b_policy_default_params(C.byref(p)), "g1b_policy_default_params")
+    return p
+
+
+def policy_sizes():
+    v = [C.c_int() for _ in range(4)]
+    check(lib().g1b_policy_sizes(*[C.byref(x) for x in v]), "g1b_policy_sizes")
+    return tuple(x.value for x in v)
+
+
+def policy_status():
+    """Device status of the policy kernels (synchronises); 0 = ok.  Clears it."""
+    code = C.c_int()
+    check(lib().g1b_policy_status(C.byref(code)), "g1b_policy_status")
+    return code.value

@@ -431,8 +431,11 @@ G1_HD SV bias_force(const AI& In, const V3& w, const V3& v, const V3& g) {
 }
 
 // ---------------------------------------------------------------- scratch
-// Per hinge h (body h + 1), slot h * 11 + k:
-//   0 q, 1 qd, 2 cos q, 3 sin q, 4-9 U / D (backward -> forward), 10 u / D.
+// Per hinge h (body h + 1), 11 slots: k = 0 q (slot h), 1 qd (slot 29 + h),
+// and k = 2..10 at slot 58 + 9 h + (k - 2): 2 cos q, 3 sin q, 4-9 U / D
+// (backward -> forward), 10 u / D.  The joint state comes first so that the
+// rest of the scratch is free between substeps (the policy step reuses it
+// for its network tiles).
 // Per chain c (0 left leg, 1 right leg, 2 waist, 3 left arm, 4 right arm):
 //   kSlotChain + 9 c: twist (6) and gravity (3) of the chain's last body
 //   (FK -> backward; the backward pass recovers the other bodies' twist and
@@ -448,7 +451,10 @@ constexpr int kSlotXchg = kSlotFoot + 12;
 constexpr int kXUp = kSlotXchg, kXA0 = kSlotXchg + 27, kXBase = kSlotXchg + 33, kXReset = kSlotXchg + 46;
 constexpr int kNumSlotsSingle = kSlotXchg;  // one thread per env
 constexpr int kNumSlots = kSlotXchg + 47;   // two threads per env
-G1_CE int hslot(int body, int k) { return (body - 1) * kSlotsPerHinge + k; }
+constexpr int kSlotJointState = 2 * kNJ;  // q and qd of every hinge
+G1_CE int hslot(int body, int k) {
+  return k < 2 ? k * kNJ + (body - 1) : kSlotJointState + (body - 1) * (kSlotsPerHinge - 2) + (k - 2);
+}
 
 // ----------------------------------------------------------- env data
 // Base state kept in registers; joint angles and rates live in the scratch.

@@ -97,6 +97,95 @@ int g1b_autotune(int nenv, int nsub, void* stream, float* best_ms);
  * on the whole device; writes achieved TFLOP/s (2 flops per FFMA). */
 int g1b_ffma_peak(int iters, float* tflops, float* ms);
 
+/* ------------------------------------------------ policy-fused rollout */
+/* No reference counterpart as one call: the reference runs the same loop in
+ * Python (examples/train.py:262-325: ActorCritic.act, PD targets, pushes,
+ * G1Sim.step, get_obs, compute_reward_and_done, resets, command redraws).
+ * Here one CTA keeps 128 envs on an SM for all npolicy policy steps; the
+ * observation (src/g1sim.py:132-170) is built in shared memory, normalised
+ * (examples/train.py:68-69) and fed to the critic and actor MLPs
+ * (99-512-256-128-{1,29}, ELU; train.py:16-39) on the tensor cores (BF16
+ * operands, FP32 accumulation), then decim substeps run in the same kernel.
+ *
+ * Network weights in the kernel's layout, packed by g1sim_b200/policy.py
+ * from an ActorCritic state dict (train.py:16-47):
+ *   weights   BF16, the critic's four layers then the actor's four, each
+ *             W (out x in) zero-padded to N x K = 512x112, 256x512,
+ *             128x256, {16 | 32}x128 and stored in K-chunks of 16 / 32 /
+ *             64 / 128 columns, each chunk as [K/8][N/8][8][8]
+ *   bias      FP32, per layer padded to N (critic 912, then actor 928)
+ *   log_std   [29], the actor's `std` parameter (sigma = exp(log_std))
+ *   obs_mean, obs_var [99]: normaliser statistics, constant during a call
+ * All device pointers; weights 16-byte aligned. */
+typedef struct g1b_policy {
+  const void* weights;
+  const float* bias;
+  const float* log_std;
+  const float* obs_mean;
+  const float* obs_var;
+} g1b_policy;
+
+/* Per-env task state, SoA [.][nenv], kept by the caller across calls
+ * (examples/train.py:257-261: command_timeout, env_episode_length,
+ * push_interval; prev_actions :264). */
+typedef struct g1b_task_state {
+  float* commands;    /* [3][nenv] vx, vy (m/s), yaw rate (rad/s) */
+  float* prev_action; /* [29][nenv] raw action of the previous policy step */
+  int* cmd_timer;     /* [nenv] policy steps until the command is redrawn */
+  int* ep_len;        /* [nenv] policy steps since the last reset */
+  int* push_timer;    /* [nenv] policy steps until the next push */
+} g1b_task_state;
+
+enum { G1B_SAMPLE = 1, G1B_PUSH = 2, G1B_RESET = 4, G1B_COMMANDS = 8 };
+
+/* Task parameters; g1b_policy_default_params fills the reference values. */
+typedef struct g1b_task_params {
+  unsigned seed;                     /* RNG seed: action noise, pushes, commands */
+  int step0;                         /* global index of the call's first policy step */
+  float cmd_lo[3], cmd_hi[3];        /* command draw ranges */
+  int cmd_steps_lo, cmd_steps_hi;    /* command redraw interval, U{lo..hi-1} (150, 250) */
+  int push_steps_lo, push_steps_hi;  /* push interval (50, 150) */
+  float push_vel[6];                 /* push U(-v, v) added to qvel[0:6] */
+  int max_episode;                   /* timeout in policy steps (1000) */
+  float tilt_limit;                  /* termination tilt in rad (70 deg) */
+  unsigned reset_seed;               /* g1_cuda_reset_done seed, noise, drop (42, 0.1, 0.02) */
+  float reset_noise, reset_drop;
+  int flags;                         /* G1B_SAMPLE | G1B_PUSH | G1B_RESET | G1B_COMMANDS */
+} g1b_task_params;
+
+/* Outputs per policy step t of the call, [npolicy][nenv][...] row-major as
+ * the reference RolloutBuffer (examples/train.py:94-101); each nullable.
+ * last_obs [nenv][99] / last_value [nenv]: observation and critic value of
+ * the state after the last step (the bootstrap value, train.py:327-328). */
+typedef struct g1b_rollout_out {
+  float* obs;        /* observation the action was taken on, raw */
+  float* actions;    /* [29] sampled action (network units) */
+  float* mean;       /* [29] actor output */
+  float* logp;       /* log-probability of the action */
+  float* value;      /* critic value */
+  float* reward;     /* reward of the transition */
+  uint8_t* done;     /* termination (tilt), as buffered by the reference */
+  uint8_t* reset;    /* termination or timeout: the env was reset after the step */
+  float* last_obs;
+  float* last_value;
+} g1b_rollout_out;
+
+int g1b_policy_default_params(g1b_task_params* out);
+/* Sizes of the packed network: weight bytes, bias floats, obs and action dims. */
+int g1b_policy_sizes(int* weight_bytes, int* bias_floats, int* obs_dim, int* act_dim);
+/* npolicy policy steps of decim substeps each, on the caller's stream.
+ * foot_pos, foot_vel, contact_forces are required (the reward reads them)
+ * and hold the last substep's values on return.  npolicy = 0 with
+ * last_obs / last_value set evaluates the current state only. */
+int g1b_policy_rollout(int nenv, int npolicy, int decim, const g1b_config* cfg, const g1b_task_params* tp,
+                       const g1b_policy* pol, float* qpos, float* qvel, float* anchor, float* ctrl,
+                       const float* mu, const float* dmass, const g1b_task_state* ts, const g1b_rollout_out* out,
+                       float* foot_pos, float* foot_vel, float* contact_forces, void* stream);
+/* Device-side status of the policy kernels since the last call (reads a
+ * device flag, synchronising the device): 0 ok, 1 a tensor-core pipeline
+ * wait timed out and the affected CTAs stopped early.  Clears the flag. */
+int g1b_policy_status(int* code);
+
 #ifdef __cplusplus
 }
 #endif
