@@ -802,7 +802,8 @@ int g1b_policy_rollout(int nenv, int npolicy, int decim, const g1b_config* cfg, 
   if (!cfg || !tp || !pol || !ts || !out) return fail("policy_rollout: cfg, params, policy, state, out required");
   if (!pol->weights || !pol->bias || !pol->log_std || !pol->obs_mean || !pol->obs_var)
     return fail("policy_rollout: every policy array is required");
-  if (((uintptr_t)pol->weights) & 15) return fail("policy_rollout: weights must be 16-byte aligned");
+  if ((((uintptr_t)pol->weights) | ((uintptr_t)pol->bias)) & 15)
+    return fail("policy_rollout: weights and bias must be 16-byte aligned");
   if (!ts->commands || !ts->prev_action || !ts->cmd_timer || !ts->ep_len || !ts->push_timer)
     return fail("policy_rollout: every task-state array is required");
   if (!foot_pos || !foot_vel || !contact_forces)

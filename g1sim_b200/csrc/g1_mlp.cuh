@@ -26,7 +26,7 @@ namespace g1b::tc {
 
 constexpr int kRows = 128;          // rows of every MMA / TMEM lanes used
 constexpr int kStageBytes = 16384;  // one weight chunk
-constexpr int kStages = 3;          // weight ring depth
+constexpr int kStages = 4;          // weight ring depth = loader threads
 constexpr int kTmemCols = 512;      // whole tensor memory of the SM (one CTA per SM)
 
 enum Act : int { kNone = 0, kElu = 1, kSilu = 2 };
@@ -58,6 +58,18 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Non-blocking test of the same condition.
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(bar), "r"(parity)
@@ -133,6 +145,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 consecutive FP32 columns of this thread's TMEM lane, one wait.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // ------------------------------------------------------- tile layout
 // Byte offset of element (row, k) in a [K/8][R/8][8][8] BF16 tile.
 template <int R = kRows>
@@ -153,9 +182,12 @@ __device__ __forceinline__ void st_row8(uint8_t* tile, int row, int k8, const fl
   *reinterpret_cast<uint4*>(tile + tile_off(row, k8)) = w;
 }
 
+// Hidden activations.  The result is rounded to BF16 (8 significant bits)
+// for the next layer, so the hardware exponential (ex2.approx, relative
+// error ~2^-22) is far inside that rounding.
 __device__ __forceinline__ float activate(float x, int act) {
-  if (act == kElu) return x > 0.0f ? x : expm1f(x);
-  if (act == kSilu) return x / (1.0f + expf(-x));
+  if (act == kElu) return x > 0.0f ? x : __expf(x) - 1.0f;
+  if (act == kSilu) return __fdividef(x, 1.0f + __expf(-x));
   return x;
 }
 
@@ -210,17 +242,25 @@ struct Chain {
   }
 };
 
-// Per-CTA pipeline state.  Every thread holds a copy; the chunk counters
-// advance only in the issuing thread (thread 0), the accumulator phase in
-// all threads (each waits on every layer's completion).
+// Per-CTA pipeline state.  Every thread holds a copy.  Weight copies are
+// issued by kStages loader threads (lane 0 of warps 0..kStages-1), loader j
+// owning ring stage j and therefore the chunks g = j (mod kStages) of the
+// global chunk sequence.  Bulk copies issued by one thread complete one after
+// another (about 0.3 us each on B200 whatever their size up to 64 KB, measured),
+// while copies of different threads overlap; four issuers keep the stream
+// near the L2 -> SM rate.  Thread 0 (loader 0) also issues the MMAs.
+// Loaders issue their next copy whenever they wait anyway (for a chunk to
+// land or for a layer to finish) and its stage has been released by the MMAs
+// of the chunk kStages earlier.
 struct Pipe {
   uint32_t act;      // shared address of the A tile
   uint32_t stage;    // shared address of stage 0
   uint32_t bar;      // shared address of the barriers: full[kStages], empty[kStages], acc
   uint32_t tmem;     // tensor-memory base address
-  uint32_t loaded;   // chunks whose copy was issued (thread 0)
-  uint32_t issued;   // chunks whose MMAs were issued (thread 0)
-  uint32_t base;     // global index of chunk 0 of the current pass (thread 0)
+  uint32_t loaded;   // loader: global index of the next chunk it copies
+  uint32_t issued;   // thread 0: chunks whose MMAs were issued
+  uint32_t base;     // global index of chunk 0 of the current pass
+  uint32_t passes;   // passes begun
   uint32_t acc_n;    // accumulator completions waited for (all threads)
   __device__ uint32_t full(int s) const { return bar + 8u * s; }
   __device__ uint32_t empty(int s) const { return bar + 8u * (kStages + s); }
@@ -228,20 +268,32 @@ struct Pipe {
 };
 constexpr int kBarriers = 2 * kStages + 1;
 
-// Barrier initialisation (one thread), before the CTA's first barrier sync.
-__device__ __forceinline__ void pipe_init(const Pipe& p) {
-  for (int s = 0; s < kStages; ++s) {
-    mbar_init(p.full(s), 1);
-    mbar_init(p.empty(s), 1);
+// Loader index of this thread (lane 0 of warps 0..kStages-1), or -1.
+__device__ __forceinline__ int loader_id() {
+  return ((threadIdx.x & 31) == 0 && (threadIdx.x >> 5) < kStages) ? (int)(threadIdx.x >> 5) : -1;
+}
+
+// Every thread, before its first use of the pipe; thread 0 also initialises
+// the barriers (before the CTA's first barrier sync).
+__device__ __forceinline__ void pipe_init(Pipe& p) {
+  const int j = loader_id();
+  p.loaded = j >= 0 ? (uint32_t)j : 0u;
+  p.issued = p.base = p.passes = p.acc_n = 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(p.full(s), 1);
+      mbar_init(p.empty(s), 1);
+    }
+    mbar_init(p.accb(), 1);
+    mbar_fence_init();
   }
-  mbar_init(p.accb(), 1);
-  mbar_fence_init();
 }
 
 template <class Net>
 struct Runner {
   using C = Chain<Net>;
   static_assert(C::valid(), "layer shapes must fit the UMMA / staging constraints");
+  static_assert(C::kChunks % kStages == 0, "loader j owns the chunks j (mod kStages) of every pass");
 
   // Offset and size of pass chunk c, from compile-time layer data.
   template <int L = 0>
@@ -257,25 +309,40 @@ struct Runner {
       chunk_info<L + 1>(c, off, bytes);
     }
   }
-  // Issue the copy of pass chunk c (thread 0).  Returns false on a timeout.
-  static __device__ bool load(Pipe& p, const uint8_t* blob, int c) {
+  // Loader threads: issue this loader's next copy of the pass if its stage
+  // has been released (non-blocking).
+  static __device__ __forceinline__ void service(Pipe& p, const uint8_t* blob) {
+    const int j = loader_id();
+    if (j < 0) return;
     const uint32_t g = p.loaded;
-    const int s = (int)(g % kStages);
-    if (g >= (uint32_t)kStages && !mbar_wait(p.empty(s), ((g / kStages) - 1) & 1)) return false;
+    const int c = (int)(g - p.base);
+    if (c >= C::kChunks) return;
+    if (g >= (uint32_t)kStages && !mbar_test(p.empty(j), ((g / kStages) - 1) & 1)) return;
     uint32_t off = 0, bytes = 0;
     chunk_info(c, off, bytes);
-    mbar_expect_tx(p.full(s), bytes);
-    bulk_g2s(p.stage + (uint32_t)s * kStageBytes, blob + off, bytes, p.full(s));
-    ++p.loaded;
+    mbar_expect_tx(p.full(j), bytes);
+    bulk_g2s(p.stage + (uint32_t)j * kStageBytes, blob + off, bytes, p.full(j));
+    p.loaded += kStages;
+  }
+  // Every thread: start a pass over the whole chain (loaders copy their
+  // first chunk; every stage is free between passes).
+  static __device__ bool begin(Pipe& p, const uint8_t* blob) {
+    p.base = p.passes * (uint32_t)C::kChunks;
+    ++p.passes;
+    service(p, blob);
     return true;
   }
-  // Start a pass over the whole chain: prefetch the first kStages chunks.
-  static __device__ bool begin(Pipe& p, const uint8_t* blob) {
-    if (threadIdx.x != 0) return true;
-    p.base = p.loaded;
-    for (int c = 0; c < kStages && c < C::kChunks; ++c)
-      if (!load(p, blob, c)) return false;
-    return true;
+  // Thread 0: wait until chunk g has landed, serving its own loads meanwhile.
+  static __device__ bool wait_chunk(Pipe& p, const uint8_t* blob, uint32_t g) {
+    const int s = (int)(g % kStages);
+    const uint32_t par = (g / kStages) & 1;
+    if (mbar_test(p.full(s), par)) return true;
+    const uint64_t t0 = globaltimer();
+    for (;;) {
+      service(p, blob);
+      if (mbar_test(p.full(s), par)) return true;
+      if (globaltimer() - t0 > kWaitNs) return false;
+    }
   }
   // Issue the MMAs of layer L (thread 0); its accumulator occupies TMEM
   // columns [0, N).  The A tile must be complete and fenced.
@@ -291,7 +358,7 @@ struct Runner {
     for (int c = 0; c < C::chunks(L); ++c) {
       const uint32_t g = p.issued;
       const int s = (int)(g % kStages);
-      if (!mbar_wait(p.full(s), (g / kStages) & 1)) return false;
+      if (!wait_chunk(p, blob, g)) return false;
       const uint32_t bstage = p.stage + (uint32_t)s * kStageBytes;
 #pragma unroll
       for (int j = 0; j < ksteps; ++j) {
@@ -305,23 +372,66 @@ struct Runner {
       }
       mma_commit(p.empty(s));
       ++p.issued;
-      // keep kStages - 1 chunks in flight behind the one just issued
-      while (p.loaded < p.issued + (uint32_t)kStages - 1 && (int)(p.loaded - p.base) < C::kChunks)
-        if (!load(p, blob, (int)(p.loaded - p.base))) return false;
+      service(p, blob);
     }
     mma_commit(p.accb());
     return true;
   }
-  // Every thread: wait for layer completion, then make TMEM reads safe.
-  static __device__ bool wait_acc(Pipe& p) {
-    const bool ok = mbar_wait(p.accb(), p.acc_n & 1);
+  // Every thread: wait for the layer's accumulator (loaders keep copying
+  // meanwhile, and once more when it completes since the layer's MMAs have
+  // then released every stage), then make TMEM reads safe.
+  static __device__ bool wait_acc(Pipe& p, const uint8_t* blob) {
+    const uint32_t par = p.acc_n & 1;
     ++p.acc_n;
+    bool ok = true;
+    if (!mbar_test(p.accb(), par)) {
+      const uint64_t t0 = globaltimer();
+      for (;;) {
+        service(p, blob);
+        if (mbar_test(p.accb(), par)) break;
+        if (globaltimer() - t0 > kWaitNs) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    service(p, blob);
     tc_fence_after();
     return ok;
   }
-  // Every thread: bias + activation of layer l's accumulator into the A tile
-  // of layer l+1.  Warp w reads TMEM lanes 32*(w%4).. and the column half w/4
-  // (kThreads = 256) or all columns (kThreads = 128).
+  // After an abort: loaders wait (bounded) for their last copy, thread 0 for
+  // its last MMAs, so nothing writes the CTA's memory once it has left.
+  static __device__ void drain(const Pipe& p) {
+    const int j = loader_id();
+    if (j >= 0 && p.loaded >= (uint32_t)kStages) {
+      const uint32_t g = p.loaded - kStages;
+      mbar_wait(p.full(j), (g / kStages) & 1);
+    }
+    if (threadIdx.x == 0 && p.issued > 0) {
+      const uint32_t g = p.issued - 1;
+      mbar_wait(p.empty((int)(g % kStages)), (g / kStages) & 1);
+    }
+  }
+  // bias + activation of 32 accumulator columns, stored as BF16 at (row, c..c+31)
+  template <int kAct>
+  static __device__ __forceinline__ void finish32(const float (&r)[32], const float* bias, uint8_t* act_tile,
+                                                  int row, int c) {
+    float v[32];
+    const float4* b4 = reinterpret_cast<const float4*>(bias);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float4 b = __ldg(b4 + i);
+      v[4 * i + 0] = activate(r[4 * i + 0] + b.x, kAct);
+      v[4 * i + 1] = activate(r[4 * i + 1] + b.y, kAct);
+      v[4 * i + 2] = activate(r[4 * i + 2] + b.z, kAct);
+      v[4 * i + 3] = activate(r[4 * i + 3] + b.w, kAct);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) st_row8(act_tile, row, c + 8 * i, v + 8 * i);
+  }
+  // Every thread: bias + activation of layer L's accumulator into the A tile
+  // of layer L+1.  Warp w reads TMEM lanes 32*(w%4).. and the column half w/4
+  // (kThreads = 256) or all columns (kThreads = 128).  bias: 16-byte aligned.
   template <int L, int kThreads>
   static __device__ void epilogue(const Pipe& p, uint8_t* act_tile, const float* bias) {
     constexpr Layer Ly = Net::layer[L];
@@ -329,16 +439,14 @@ struct Runner {
     const int row = q * 32 + (threadIdx.x & 31);
     constexpr int kHalves = kThreads / 128;
     constexpr int span = Ly.N / kHalves;
-    static_assert(span % 16 == 0, "epilogue columns come in groups of 16");
+    static_assert(span % 32 == 0, "epilogue columns come in groups of 32");
     const int c0 = (warp >> 2) * span;
     const uint32_t lane_base = p.tmem + ((uint32_t)(q * 32) << 16);
-    for (int c = c0; c < c0 + span; c += 16) {
-      float v[16];
-      tmem_ld16(lane_base + (uint32_t)c, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = activate(v[i] + __ldg(bias + c + i), Ly.act);
-      st_row8(act_tile, row, c, v);
-      st_row8(act_tile, row, c + 8, v + 8);
+#pragma unroll 1
+    for (int c = c0; c < c0 + span; c += 32) {
+      float v[32];
+      tmem_ld32(lane_base + (uint32_t)c, v);
+      finish32<Ly.act>(v, bias + c, act_tile, row, c);
     }
   }
 };

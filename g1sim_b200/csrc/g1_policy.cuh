@@ -45,9 +45,11 @@ using PolicyRun = tc::Runner<PolicyNet>;
 constexpr int kPolicyEnvs = 128;
 constexpr uint32_t kPolicyActOff = (uint32_t)kSlotJointState * kPolicyEnvs * 4;  // after q, qd
 constexpr uint32_t kPolicyStageOff = kPolicyActOff + PolicyChain::kActBytes;
-constexpr size_t kPolicySmem = (size_t)kNumSlots * kPolicyEnvs * sizeof(float);
-static_assert(kPolicyStageOff + tc::kStages * tc::kStageBytes <= kPolicySmem,
-              "network tiles must fit in the step scratch");
+// The step scratch, extended where the weight ring reaches past it.
+constexpr size_t kPolicyScratch = (size_t)kNumSlots * kPolicyEnvs * sizeof(float);
+constexpr size_t kPolicyRingEnd = (size_t)kPolicyStageOff + (size_t)tc::kStages * tc::kStageBytes;
+constexpr size_t kPolicySmem = kPolicyScratch > kPolicyRingEnd ? kPolicyScratch : kPolicyRingEnd;
+static_assert(kPolicySmem + 4096 <= 232448, "dynamic + static shared memory must fit one CTA");
 static_assert(kPolicyActOff % 16 == 0 && kPolicyStageOff % 16 == 0, "operand tiles need 16-byte alignment");
 
 enum : int { kFlagSample = 1, kFlagPush = 2, kFlagReset = 4, kFlagCommands = 8 };
@@ -142,10 +144,13 @@ __device__ __forceinline__ float obs_joint_col(int c, const Scr& scr, const floa
 }
 
 // Writes columns [8 g0, 8 g1) of this env's observation row: normalised and
-// BF16 into the A tile, raw FP32 into raw_row (nullable).
+// BF16 into the A tile, raw FP32 into raw_row (nullable).  The normalisation
+// (reference examples/train.py:68-69) multiplies by the reciprocal standard
+// deviation computed once per CTA; norm: [0, 112) mean, [112, 224)
+// 1 / sqrt(var + 1e-8), in shared memory.
 template <int G0, int G1, class Scr>
 __device__ __forceinline__ void build_obs_cols(uint8_t* tile, int row, const float* base12, const Scr& scr,
-                                               const float* ctrl_e, size_t n, const PolicyArgs& pa,
+                                               const float* ctrl_e, size_t n, const float* norm,
                                                float* raw_row) {
 #pragma unroll
   for (int g = G0; g < G1; ++g) {
@@ -160,7 +165,7 @@ __device__ __forceinline__ void build_obs_cols(uint8_t* tile, int row, const flo
         o = obs_joint_col(c, scr, ctrl_e, n);
       if (c < kObs) {
         if (raw_row) raw_row[c] = o;
-        const float z = __fdiv_rn(__fsub_rn(o, __ldg(pa.obs_mean + c)), sqrtf(__fadd_rn(__ldg(pa.obs_var + c), 1e-8f)));
+        const float z = __fmul_rn(__fsub_rn(o, norm[c]), norm[kObsPad + c]);
         v[i] = fminf(fmaxf(z, -5.0f), 5.0f);
       } else {
         v[i] = 0.0f;
@@ -265,6 +270,7 @@ struct PolicyShared {
   uint32_t tmem;
   int abort;
   float xch[3][kPolicyEnvs];  // 0: logp of the upper joints, 1: their action change, 2: reset flag
+  float norm[2 * kObsPad];     // observation mean, reciprocal standard deviation
 };
 
 // Observation rows of the CTA's tile into the A tile: role 0 writes columns
@@ -272,18 +278,18 @@ struct PolicyShared {
 template <class Scr>
 __device__ __forceinline__ void policy_obs_tile(uint8_t* tile, int role, int le, bool act_env, const EnvState& st,
                                                 const Scr& scr, int e, size_t n, const float* ctrl,
-                                                const PolicyArgs& pa, const TaskArgs& ta, float* raw_row) {
+                                                const float* norm, const TaskArgs& ta, float* raw_row) {
   if (act_env) {
     const float* ctrl_e = ctrl + e;
     float base12[12];
     if (role == 0) {
       const float cmd[3] = {ta.cmd[e], ta.cmd[n + e], ta.cmd[2 * n + e]};
       obs_base(st, cmd, base12);
-      build_obs_cols<0, 6>(tile, le, base12, scr, ctrl_e, n, pa, raw_row);
+      build_obs_cols<0, 6>(tile, le, base12, scr, ctrl_e, n, norm, raw_row);
     } else {
 #pragma unroll
       for (int i = 0; i < 12; ++i) base12[i] = 0.0f;
-      build_obs_cols<6, kObsPad / 8>(tile, le, base12, scr, ctrl_e, n, pa, raw_row);
+      build_obs_cols<6, kObsPad / 8>(tile, le, base12, scr, ctrl_e, n, norm, raw_row);
     }
   } else {
     const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -308,31 +314,51 @@ __device__ __forceinline__ bool policy_layer_done(PolicyShared& ps, bool ok) {
 template <int L>
 __device__ __forceinline__ bool policy_hidden(tc::Pipe& p, PolicyShared& ps, uint8_t* tile, const PolicyArgs& pa) {
   bool ok = PolicyRun::issue<L>(p, pa.w);
-  ok = PolicyRun::wait_acc(p) && ok;
+  ok = PolicyRun::wait_acc(p, pa.w) && ok;
   PolicyRun::epilogue<L, 2 * kPolicyEnvs>(p, tile, pa.b + PolicyChain::bias_off(L));
   return policy_layer_done(ps, ok);
 }
 
+// Copy nrows rows of `width` floats from shared staging to contiguous global
+// rows, consecutive threads on consecutive floats (coalesced).
+__device__ __forceinline__ void copy_rows(float* dst, const float* src, int nrows, int width) {
+  const int total = nrows * width;
+  for (int i = threadIdx.x; i < total; i += 2 * kPolicyEnvs) dst[i] = src[i];
+}
+
+// Shared staging of the raw observation rows [128][99] inside the activation
+// region, past the observation tile (28,672 bytes).
+constexpr uint32_t kRawObsOff = kPolicyActOff + 32768;
+static_assert(32768 >= kObsPad / 8 * (kPolicyEnvs / 8) * 128, "observation tile below the raw staging");
+static_assert(32768 + kPolicyEnvs * kObs * 4 <= PolicyChain::kActBytes, "raw staging inside the region");
+
 // One network pass (critic, then actor) for the CTA's tile; every thread
-// calls it.  Role 0 threads hold the base state; the raw observation is
-// written once (raw_row, nullable).  value: the critic output (role 0);
-// out32: actor pre-bias outputs, columns 0-15 (both roles) and 16-31 (role 1).
-// Returns false when the CTA must stop (a wait gave up).
+// calls it.  Role 0 threads hold the base state.  raw_dst (nullable): global
+// rows of this tile's raw observation (nrows of them), written once through
+// shared staging.  value: the critic output (role 0); out32: actor pre-bias
+// outputs, columns 0-15 (both roles) and 16-31 (role 1).  Returns false when
+// the CTA must stop (a wait gave up).
 template <class Scr>
 __device__ bool policy_pass(tc::Pipe& p, PolicyShared& ps, uint8_t* smraw, int role, int le, bool act_env,
                             const EnvState& st, const Scr& scr, int e, size_t n, const float* ctrl,
-                            const PolicyArgs& pa, const TaskArgs& ta, float* raw_row, float& value,
+                            const PolicyArgs& pa, const TaskArgs& ta, float* raw_dst, int nrows, float& value,
                             float (&out32)[32]) {
   uint8_t* tile = smraw + kPolicyActOff;
+  float* raw_sm = reinterpret_cast<float*>(smraw + kRawObsOff);
   const uint32_t lane = p.tmem + ((uint32_t)((threadIdx.x >> 5) & 3) * 32u << 16);
   bool ok = PolicyRun::begin(p, pa.w);
   // critic
-  policy_obs_tile(tile, role, le, act_env, st, scr, e, n, ctrl, pa, ta, raw_row);
+  policy_obs_tile(tile, role, le, act_env, st, scr, e, n, ctrl, ps.norm, ta, raw_dst ? raw_sm + le * kObs : nullptr);
   if (!policy_layer_done(ps, ok)) return false;
-  if (!policy_hidden<0>(p, ps, tile, pa) || !policy_hidden<1>(p, ps, tile, pa) || !policy_hidden<2>(p, ps, tile, pa))
-    return false;
+  ok = PolicyRun::issue<0>(p, pa.w);
+  if (raw_dst) copy_rows(raw_dst, raw_sm, nrows, kObs);  // block-uniform; runs under the MMAs
+  ok = PolicyRun::wait_acc(p, pa.w) && ok;
+  if (raw_dst) __syncthreads();  // the epilogue below overwrites the staging
+  PolicyRun::epilogue<0, 2 * kPolicyEnvs>(p, tile, pa.b + PolicyChain::bias_off(0));
+  if (!policy_layer_done(ps, ok)) return false;
+  if (!policy_hidden<1>(p, ps, tile, pa) || !policy_hidden<2>(p, ps, tile, pa)) return false;
   ok = PolicyRun::issue<3>(p, pa.w);
-  ok = PolicyRun::wait_acc(p) && ok;
+  ok = PolicyRun::wait_acc(p, pa.w) && ok;
   if (role == 0) {
     float v[16];
     tc::tmem_ld16(lane, v);
@@ -340,12 +366,12 @@ __device__ bool policy_pass(tc::Pipe& p, PolicyShared& ps, uint8_t* smraw, int r
   }
   if (!policy_layer_done(ps, ok)) return false;
   // actor (the observation tile is rebuilt: the hidden layers overwrote it)
-  policy_obs_tile(tile, role, le, act_env, st, scr, e, n, ctrl, pa, ta, nullptr);
+  policy_obs_tile(tile, role, le, act_env, st, scr, e, n, ctrl, ps.norm, ta, nullptr);
   if (!policy_layer_done(ps, true)) return false;
   if (!policy_hidden<4>(p, ps, tile, pa) || !policy_hidden<5>(p, ps, tile, pa) || !policy_hidden<6>(p, ps, tile, pa))
     return false;
   ok = PolicyRun::issue<7>(p, pa.w);
-  ok = PolicyRun::wait_acc(p) && ok;
+  ok = PolicyRun::wait_acc(p, pa.w) && ok;
   {
     float v[16];
     tc::tmem_ld16(lane, v);
@@ -358,16 +384,6 @@ __device__ bool policy_pass(tc::Pipe& p, PolicyShared& ps, uint8_t* smraw, int r
     }
   }
   return policy_layer_done(ps, ok);
-}
-
-// Thread 0 after an abort: wait (bounded) for the copies and MMAs in flight.
-__device__ void policy_drain(tc::Pipe& p) {
-  if (threadIdx.x != 0) return;
-  for (uint32_t g = p.issued; g < p.loaded; ++g) tc::mbar_wait(p.full((int)(g % tc::kStages)), (g / tc::kStages) & 1);
-  if (p.issued > 0) {
-    const uint32_t g = p.issued - 1;
-    tc::mbar_wait(p.empty((int)(g % tc::kStages)), (g / tc::kStages) & 1);
-  }
 }
 
 __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
@@ -386,10 +402,12 @@ __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
   p.act = tc::smem_u32(smraw + kPolicyActOff);
   p.stage = tc::smem_u32(smraw + kPolicyStageOff);
   p.bar = tc::smem_u32(ps.bars);
-  p.loaded = p.issued = p.base = p.acc_n = 0;
-  if (threadIdx.x == 0) {
-    tc::pipe_init(p);
-    ps.abort = 0;
+  tc::pipe_init(p);
+  if (threadIdx.x == 0) ps.abort = 0;
+  if (threadIdx.x < kObsPad) {
+    const int c = threadIdx.x;
+    ps.norm[c] = c < kObs ? __ldg(pa.obs_mean + c) : 0.0f;
+    ps.norm[kObsPad + c] = c < kObs ? __fdiv_rn(1.0f, sqrtf(__fadd_rn(__ldg(pa.obs_var + c), 1e-8f))) : 0.0f;
   }
   if (threadIdx.x < 32) tc::tmem_alloc(tc::smem_u32(&ps.tmem), tc::kTmemCols);
   tc::tc_fence_before();
@@ -430,9 +448,12 @@ __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
       const size_t row = final_eval ? (size_t)e : (size_t)k * sd + (size_t)e;
       float value = 0.0f;
       float v32[32];
-      float* raw_row = final_eval ? (out.last_obs && act ? out.last_obs + (size_t)e * kObs : nullptr)
-                                  : (out.obs && act ? out.obs + row * kObs : nullptr);
-      if (!policy_pass(p, ps, smraw, role, le, act, st, scr, e, sd, ctrl, pa, ta, raw_row, value, v32)) {
+      const size_t e0 = (size_t)tile * ENVS;
+      const int nrows = n - (int)e0 < ENVS ? n - (int)e0 : ENVS;
+      const size_t row0 = final_eval ? e0 : (size_t)k * sd + e0;  // first output row of the tile
+      float* raw_dst = final_eval ? (out.last_obs ? out.last_obs + e0 * kObs : nullptr)
+                                  : (out.obs ? out.obs + row0 * kObs : nullptr);
+      if (!policy_pass(p, ps, smraw, role, le, act, st, scr, e, sd, ctrl, pa, ta, raw_dst, nrows, value, v32)) {
         stop = true;
         break;
       }
@@ -442,9 +463,12 @@ __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
       }
       // ---- action, log-probability, targets, push
       float lp = 0.0f, ar = 0.0f;
+      // action and mean rows staged in shared memory, copied out coalesced
+      float* act_sm = reinterpret_cast<float*>(smraw + kPolicyActOff);
+      float* mean_sm = act_sm + ENVS * kNU;
       if (act) {
-        float* act_row = out.act ? out.act + row * kNU : nullptr;
-        float* mean_row = out.mean ? out.mean + row * kNU : nullptr;
+        float* act_row = out.act ? act_sm + le * kNU : nullptr;
+        float* mean_row = out.mean ? mean_sm + le * kNU : nullptr;
         if (role == 0) {
           lp = sample_actions<0, 12, 0>(v32, pa, tp, e, stp, ctrl + e, sd, ta, act_row, mean_row, ar);
           if (out.value) out.value[row] = value;
@@ -475,6 +499,11 @@ __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
       if (act && role == 0) {
         ar += ps.xch[1][le];
         if (out.logp) out.logp[row] = lp + ps.xch[0][le];
+      }
+      if (out.act || out.mean) {  // block-uniform
+        if (out.act) copy_rows(out.act + row0 * kNU, act_sm, nrows, kNU);
+        if (out.mean) copy_rows(out.mean + row0 * kNU, mean_sm, nrows, kNU);
+        __syncthreads();  // the substeps reuse the staging
       }
       // ---- physics: decim substeps of the split step
       for (int s = 0; s < decim; ++s) {
@@ -605,7 +634,7 @@ __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
     if (stop) break;
   }
   __syncthreads();
-  if (stop) policy_drain(p);
+  if (stop) PolicyRun::drain(p);
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();

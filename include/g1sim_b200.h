@@ -116,7 +116,7 @@ int g1b_ffma_peak(int iters, float* tflops, float* ms);
  *   bias      FP32, per layer padded to N (critic 912, then actor 928)
  *   log_std   [29], the actor's `std` parameter (sigma = exp(log_std))
  *   obs_mean, obs_var [99]: normaliser statistics, constant during a call
- * All device pointers; weights 16-byte aligned. */
+ * All device pointers; weights and bias 16-byte aligned. */
 typedef struct g1b_policy {
   const void* weights;
   const float* bias;
