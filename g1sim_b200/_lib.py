@@ -54,6 +54,11 @@ class RolloutOut(C.Structure):
 
 SAMPLE, PUSH, RESET, COMMANDS = 1, 2, 4, 8
 
+
+class AdjointProblem(C.Structure):
+    """g1b_adjoint_problem."""
+    _fields_ = [("horizon", C.c_int), ("checkpoint", C.c_int), ("z_ref", C.c_float), ("w_track", C.c_float)]
+
 _vp = C.c_void_p
 
 
@@ -85,6 +90,9 @@ def lib():
                                       C.POINTER(Policy)] + [_vp] * 6 +
                                      [C.POINTER(TaskState), C.POINTER(RolloutOut)] + [_vp] * 4)
     L.g1b_policy_status.argtypes = [C.POINTER(C.c_int)]
+    L.g1b_adjoint_scratch_size.argtypes = [C.c_int, C.POINTER(AdjointProblem), C.POINTER(C.c_size_t)]
+    for name in ("g1b_adjoint", "g1b_adjoint_f64"):
+        getattr(L, name).argtypes = [C.c_int, C.POINTER(Config), C.POINTER(AdjointProblem)] + [_vp] * 14
     _lib = L
     return L
 

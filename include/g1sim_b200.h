@@ -186,6 +186,41 @@ int g1b_policy_rollout(int nenv, int npolicy, int decim, const g1b_config* cfg, 
  * wait timed out and the affected CTAs stopped early.  Clears the flag. */
 int g1b_policy_status(int* code);
 
+/* ------------------------------------------------------ horizon adjoint */
+/* No reference counterpart: the reference has no derivatives.  Gradient of
+ *   L = sum_{t=1..H} (qpos_t[2] - z_ref)^2 + w_track * |qpos_t[7:36] - u_{t-1}|^2
+ * over H single-substep steps x_{t+1} = step(x_t, u_t, kp_scale, kd_scale)
+ * (x = qpos, qvel, anchor; friction 1, no base-mass offset), with respect
+ * to the PD targets u_t, the per-env gain scales and the initial state.
+ * Reverse sweep with checkpoints every `checkpoint` steps and recomputation
+ * in between; each step's vector-Jacobian product is exact to rounding (the
+ * derivative of the step as computed, one-sided at contact / clamp
+ * switches). */
+typedef struct g1b_adjoint_problem {
+  int horizon;     /* H */
+  int checkpoint;  /* keep the state every `checkpoint` steps */
+  float z_ref;     /* base-height reference (0.78) */
+  float w_track;   /* weight of the joint tracking term (0.1) */
+} g1b_adjoint_problem;
+/* Scratch elements (float, or double for the _f64 variant) that g1b_adjoint
+ * needs for nenv envs: ((ceil(H/C) + 1) * 87 + C * 87 + 87 + 120) * nenv. */
+int g1b_adjoint_scratch_size(int nenv, const g1b_adjoint_problem* pr, size_t* count);
+/* Arrays SoA with the env axis fastest: qpos0 [36][nenv], qvel0 [35][nenv],
+ * anchor0 [16][nenv], targets / grad_targets [H][29][nenv], kp_scale,
+ * kd_scale, loss, grad_kp, grad_kd [nenv] (scales nullable = 1, gain and
+ * initial-state gradients nullable), grad_qpos0 [36][nenv], grad_qvel0
+ * [35][nenv]; scratch: g1b_adjoint_scratch_size elements, caller-owned. */
+int g1b_adjoint(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* pr, const float* qpos0,
+                const float* qvel0, const float* anchor0, const float* targets, const float* kp_scale,
+                const float* kd_scale, float* loss, float* grad_targets, float* grad_kp, float* grad_kd,
+                float* grad_qpos0, float* grad_qvel0, float* scratch, void* stream);
+/* The same computation in FP64 on the device (validation build: every array
+ * double, cfg converted). */
+int g1b_adjoint_f64(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* pr, const double* qpos0,
+                    const double* qvel0, const double* anchor0, const double* targets, const double* kp_scale,
+                    const double* kd_scale, double* loss, double* grad_targets, double* grad_kp, double* grad_kd,
+                    double* grad_qpos0, double* grad_qvel0, double* scratch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
