@@ -909,6 +909,68 @@ int g1b_adjoint_f64(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* 
                               grad_targets, grad_kp, grad_kd, grad_qpos0, grad_qvel0, scratch, stream);
 }
 
+}  // extern "C"
+
+// ------------------------------------------- adjoint without allocation
+// Some callers cannot call cudaMalloc (a real-time control loop that reserves
+// all device memory at start-up, or a process whose device memory belongs to
+// another allocator and that cannot hand this library a buffer).  For them,
+// g1b_adjoint_noalloc runs the FP32 horizon adjoint with its workspace in
+// this fixed device array instead of caller scratch.  Every device that
+// loads the library holds the array until the process exits.
+constexpr size_t kNoAllocScratchFloats = size_t(1) << 21;  // 8 MiB of float
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+
+namespace {
+// Device address of the array, looked up once per device (the host-side
+// name of a __device__ array is not a device address).
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[64] = {};
+
+int noalloc_scratch(float** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "adjoint_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail("adjoint_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint_noalloc: cudaGetSymbolAddress");
+    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+size_t g1b_adjoint_noalloc_capacity(void) { return kNoAllocScratchFloats; }
+
+int g1b_adjoint_noalloc(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* pr, const float* qpos0,
+                        const float* qvel0, const float* anchor0, const float* targets, const float* kp_scale,
+                        const float* kd_scale, float* loss, float* grad_targets, float* grad_kp, float* grad_kd,
+                        float* grad_qpos0, float* grad_qvel0, void* stream) {
+  if (nenv <= 0 || !pr || pr->horizon <= 0 || pr->checkpoint <= 0)
+    return fail("adjoint_noalloc: nenv, horizon and checkpoint must be positive");
+  const int C = pr->checkpoint < pr->horizon ? pr->checkpoint : pr->horizon;
+  const size_t need = adj_scratch_count<float>(nenv, pr->horizon, C);
+  if (need > kNoAllocScratchFloats) {
+    snprintf(g_err, sizeof(g_err),
+             "adjoint_noalloc: this problem needs %zu floats of workspace, more than the fixed %zu "
+             "(reduce nenv, the horizon or the checkpoint interval, or call g1b_adjoint with scratch)",
+             need, kNoAllocScratchFloats);
+    return -1;
+  }
+  float* scratch = nullptr;
+  if (int rc = noalloc_scratch(&scratch)) return rc;
+  // Every workspace slot is written before it is read within one call, so
+  // nothing left by an earlier call needs clearing.
+  return adjoint_impl<float>(nenv, cfg, pr, qpos0, qvel0, anchor0, targets, kp_scale, kd_scale, loss, grad_targets,
+                             grad_kp, grad_kd, grad_qpos0, grad_qvel0, scratch, stream);
+}
+
 int g1b_policy_status(int* code) {
   int v = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&v, g_policy_error, sizeof(int));

@@ -220,6 +220,25 @@ int g1b_adjoint_f64(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* 
                     const double* qvel0, const double* anchor0, const double* targets, const double* kp_scale,
                     const double* kd_scale, double* loss, double* grad_targets, double* grad_kp, double* grad_kd,
                     double* grad_qpos0, double* grad_qvel0, double* scratch, void* stream);
+/* No counterpart in the reference.  g1b_adjoint for callers that cannot
+ * allocate device memory (a real-time loop that reserves everything at
+ * start-up, or a host whose device memory is owned by another allocator
+ * and that cannot pass a buffer): the same FP32 computation, with the
+ * workspace in one fixed device array of g1b_adjoint_noalloc_capacity()
+ * floats (8 MiB; at horizon 64 and checkpoint 8 that is up to 1,243 envs)
+ * instead of caller scratch.  Larger problems are rejected with a message
+ * in g1b_last_error().  The library allocates nothing: every device that
+ * loads it holds the array until the process exits.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ * All calls on a device share the one array: calls that overlap on the GPU
+ * (other streams, other host threads) race and corrupt each other's
+ * results; serialise them. */
+size_t g1b_adjoint_noalloc_capacity(void);
+int g1b_adjoint_noalloc(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* pr, const float* qpos0,
+                        const float* qvel0, const float* anchor0, const float* targets, const float* kp_scale,
+                        const float* kd_scale, float* loss, float* grad_targets, float* grad_kp, float* grad_kd,
+                        float* grad_qpos0, float* grad_qvel0, void* stream);
 
 #ifdef __cplusplus
 }
