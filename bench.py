@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--nenv", type=int, default=NENV)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -190,6 +191,114 @@ def reference_arm(args, world, rank):
     return 0
 
 
+# ------------------------------------------------- policy-fused rollout
+# Actor and critic multiply-accumulates per env and policy step
+# (99-512-256-128-29 and 99-512-256-128-1, unpadded).
+ACTOR_MACS = 99 * 512 + 512 * 256 + 256 * 128 + 128 * 29
+CRITIC_MACS = 99 * 512 + 512 * 256 + 256 * 128 + 128 * 1
+POLICY_T = 25  # policy steps per launch (a PPO rollout's length); 4 launches = 1,000 substeps
+
+
+def policy_fused_bench(n, rank, device, stream, steps, warmup, world, local, init):
+    """The same 1,000 substeps per bench step, with the PPO actor and critic
+    evaluated inside the step kernel on the tensor cores every 10 substeps:
+    observation, sampling, targets, pushes, reward, termination and resets
+    in the kernel; every output buffer (obs, actions, log-probs, values,
+    rewards, dones) written."""
+    import torch
+    from g1sim_b200 import policy as P
+    sim = {k: init[k].clone() for k in ("qpos", "qvel", "anchor", "ctrl")}
+    for k, d in (("foot_pos", 6), ("foot_vel", 6), ("contact_forces", 8)):
+        sim[k] = torch.zeros(d, n, device=device)
+    sim0 = {k: v.clone() for k, v in sim.items()}
+    ac = P.ActorCritic().xavier_(torch.Generator().manual_seed(0))
+    packed = P.pack_policy(ac, device)
+    task = P.TaskState(n, device, seed=rank)
+    buf = P.RolloutBuffers(POLICY_T, n, device)
+    nlaunch = SUBSTEPS // (DECIM * POLICY_T)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MB > L2
+
+    def one():
+        with torch.cuda.stream(stream):
+            for k in sim:
+                sim[k].copy_(sim0[k])
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for j in range(nlaunch):
+                P.policy_rollout(sim, packed, task, buf, POLICY_T, decim=DECIM, step0=j * POLICY_T, seed=rank,
+                                 mu=init["mu"], dmass=init["dmass"], stream=stream.cuda_stream,
+                                 bootstrap=(j == nlaunch - 1))
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(warmup):
+        one()
+    barrier(world)
+    times = [one() for _ in range(steps)]
+    ms = max_over_ranks(statistics.mean(times), world, device)
+    from g1sim_b200 import _lib
+    status = _lib.policy_status()
+    env_steps = float(n) * SUBSTEPS
+    net_flops = 2.0 * (ACTOR_MACS + CRITIC_MACS) * n * (SUBSTEPS // DECIM)
+    return {"value": env_steps * world / (ms * 1e-3), "unit": "env-steps/s", "ms_per_step": ms,
+            "kernel": f"policy_kernel (128 envs per CTA, {POLICY_T} policy steps per launch, {nlaunch} launches)",
+            "network_tflops": net_flops / (ms * 1e-3) / 1e12,
+            "network_flops_per_env_policy_step": 2.0 * (ACTOR_MACS + CRITIC_MACS),
+            "outputs": "obs, actions, log-probs, values, rewards, dones, resets, bootstrap value",
+            "status": status, "finite": bool(torch.isfinite(buf.rewards).all().item())}
+
+
+# ------------------------------------------------------- horizon adjoint
+ADJ_ENVS, ADJ_H, ADJ_C = 4096, 64, 8
+
+
+def adjoint_bench(device, stream, steps, warmup, world):
+    """Loss and gradients over a 64-step horizon at dt 2 ms for 4,096 envs
+    (targets 64 x 29 and per-env kp / kd scales U[0.8, 1.2]), checkpoints
+    every 8 steps: forward rollout + reverse sweep, one g1b_adjoint call."""
+    import torch
+    from g1sim_b200 import adjoint as A
+    from g1sim_b200.model import g1_model_data as M
+    rng = np.random.default_rng(0)
+    n = ADJ_ENVS
+    stand = np.asarray(M.qpos_stand)
+    q0 = np.repeat(stand[:, None], n, axis=1)
+    q0[2] = 0.79
+    q0[7:] += rng.normal(0, 0.02, size=(29, n))
+    f = lambda x: torch.tensor(np.ascontiguousarray(x), dtype=torch.float32, device=device)  # noqa: E731
+    tg = f(stand[7:][None, :, None] + rng.normal(0, 0.05, size=(ADJ_H, 29, n)))
+    kp, kd = f(rng.uniform(0.8, 1.2, n)), f(rng.uniform(0.8, 1.2, n))
+    qp, qv, an = f(q0), f(np.zeros((35, n))), f(np.full((16, n), 1e30))
+    scratch = torch.empty(A.scratch_size(n, ADJ_H, ADJ_C), dtype=torch.float32, device=device)
+
+    def one():
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = A.horizon_adjoint(tg, kp, kd, qp, qv, an, checkpoint=ADJ_C, scratch=scratch,
+                                  stream=stream.cuda_stream)
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1), r
+
+    for _ in range(max(1, warmup)):
+        one()
+    times, r = [], None
+    for _ in range(max(1, steps)):
+        t, r = one()
+        times.append(t)
+    ms = max_over_ranks(statistics.mean(times), world, device)
+    return {"value": float(n) * ADJ_H * world / (ms * 1e-3), "unit": "env-steps/s (horizon steps differentiated)",
+            "ms_per_call": ms, "config": {"envs": n, "horizon": ADJ_H, "checkpoint": ADJ_C, "dt": DT,
+                                         "decision_variables": "targets 64x29 + kp/kd scale per env"},
+            "kernels": "adj_forward, adj_segment, adj_vjp (Dual<float,4>, 30 tangent blocks per env), adj_accum",
+            "finite": bool(torch.isfinite(r["grad_targets"]).all().item())}
+
+
 # ------------------------------------------------------------- our arm
 def ours(args, world, rank, local):
     import torch
@@ -315,6 +424,9 @@ def ours(args, world, rank, local):
     resets = int(rc.sum().item())
     finite = bool(torch.isfinite(st["qpos"]).all().item())
 
+    pol = policy_fused_bench(n, rank, device, stream, args.steps, args.warmup, world, local, init)
+    adj = adjoint_bench(device, stream, args.steps, args.warmup, world) if not args.no_adjoint else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference(args.cpu_seconds, n)
@@ -338,7 +450,10 @@ def ours(args, world, rank, local):
             "clocks": clk.summary(),
             "single_launch": {"value": env_steps / (single_ms * 1e-3), "ms": single_ms},
             "resets_last_step": resets, "finite": finite,
+            "policy_fused": pol,
         }
+        if adj is not None:
+            line["adjoint"] = adj
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))
