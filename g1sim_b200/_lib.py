@@ -90,6 +90,16 @@ def lib():
                                       C.POINTER(Policy)] + [_vp] * 6 +
                                      [C.POINTER(TaskState), C.POINTER(RolloutOut)] + [_vp] * 4)
     L.g1b_policy_status.argtypes = [C.POINTER(C.c_int)]
+    L.g1b_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,
+                                _vp]
+    L.g1b_gemm_status.argtypes = [C.POINTER(C.c_int)]
+    L.g1b_sur_act.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+    L.g1b_sur_act_bwd.argtypes = [C.c_int, C.c_int] + [_vp] * 6
+    L.g1b_sur_loss.argtypes = [C.c_int, C.c_int] + [_vp] * 8
+    L.g1b_sur_adam.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _vp]
+    L.g1b_sur_cast.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+    L.g1b_sur_features.argtypes = [C.c_int] + [_vp] * 10
+    L.g1b_sur_integrate.argtypes = [C.c_int, _vp, C.c_int, _vp, _vp, C.c_float, _vp, _vp, _vp]
     L.g1b_adjoint_scratch_size.argtypes = [C.c_int, C.POINTER(AdjointProblem), C.POINTER(C.c_size_t)]
     for name in ("g1b_adjoint", "g1b_adjoint_f64"):
         getattr(L, name).argtypes = [C.c_int, C.POINTER(Config), C.POINTER(AdjointProblem)] + [_vp] * 14

@@ -1,0 +1,213 @@
+"""Dynamics surrogate on the GPU (needs a B200).
+
+  * g1b_gemm_bf16 (tcgen05, BF16 operands, FP32 accumulation) against an FP64
+    CPU product of the same BF16 values, single pass and split over K with
+    atomics, to 1e-5 relative;
+  * the training kernels (forward, loss, backward, input gradient) against a
+    CPU FP64 restatement of the same network with the same BF16 rounding
+    points, to 3e-3 relative in 2-norm (the two sides may round a hidden
+    activation to neighbouring BF16 values when their sums differ in the
+    last bits);
+  * Adam against its published update rule on the CPU;
+  * training on transitions of the randomised workload lowers the loss;
+  * the fallback rollout with bound 0 is the exact step, bit for bit, and
+    with the trained network stays finite;
+  * across a foot touchdown the exact step's d qacc_z / d z jumps (contact
+    stiffness switching on) while the surrogate's, from its backward
+    kernels, varies smoothly -- the smooth gradient the surrogate provides.
+"""
+import numpy as np
+import pytest
+import torch
+
+from g1sim_b200 import _lib
+from g1sim_b200 import g1sim as G
+from g1sim_b200 import surrogate as S
+from g1sim_b200.model import g1_model_data as M
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+
+
+def bf(x):
+    return x.to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("M_,N,K,splits", [(256, 512, 512, 1), (128, 64, 512, 1), (384, 128, 128, 1),
+                                           (128, 512, 8192, 16), (512, 128, 4096, 8)])
+def test_gemm_matches_fp64(M_, N, K, splits):
+    g = torch.Generator(device=DEV).manual_seed(M_ + N + K)
+    A = bf(torch.randn(M_, K, device=DEV, generator=g))
+    B = bf(torch.randn(N, K, device=DEV, generator=g))
+    bias = torch.randn(N, device=DEV, generator=g)
+    C_ = torch.full((M_, N), 7.0, device=DEV)
+    S.gemm(A, B, C_, bias=bias, splits=splits)
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    ref = A.double().cpu() @ B.double().cpu().T + bias.double().cpu()
+    err = ((C_.double().cpu() - ref).norm() / ref.norm()).item()
+    assert err < 1e-5, err
+
+
+def cpu_reference(sur, X, T):
+    """FP64 restatement of forward + weighted-MSE loss + backward with the
+    kernels' BF16 rounding points (operands of every product)."""
+    r = lambda x: x.to(torch.bfloat16).double()  # noqa: E731
+    Ws = [r(w.cpu()) for w in sur.W]
+    bs = [b.cpu().double() for b in sur.b]
+    x = X.cpu().double()
+    hs, zs = [x], []
+    for i in range(5):
+        z = hs[-1] @ Ws[i].T + bs[i]
+        zs.append(z)
+        if i < 4:
+            hs.append(r(z * torch.sigmoid(z)))
+    B = X.shape[0]
+    w = sur.out_w.cpu().double()
+    e = zs[4] - T.cpu().double()
+    loss = (w * e * e).sum() / B
+    dz = r(2 * w * e / B)
+    gW, gb = [None] * 5, [None] * 5
+    gb[4] = (2 * w * e / B).sum(0)
+    for i in range(4, -1, -1):
+        gW[i] = dz.T @ hs[i]
+        if i > 0:
+            dh = dz @ Ws[i]
+            s = torch.sigmoid(zs[i - 1])
+            g = dh * s * (1 + zs[i - 1] * (1 - s))
+            gb[i - 1] = g.sum(0)
+            dz = r(g)
+        else:
+            dx = dz @ Ws[0]
+    return loss, gW, gb, dx
+
+
+def test_training_kernels_match_cpu_restatement():
+    sur = S.Surrogate(DEV, seed=1)
+    with torch.no_grad():
+        for b in sur.b:
+            b.uniform_(-0.1, 0.1)
+    g = torch.Generator(device=DEV).manual_seed(2)
+    B = 256
+    X = bf(torch.randn(B, 128, device=DEV, generator=g))
+    X[:, S.NFEAT:] = 0
+    T = torch.randn(B, 64, device=DEV, generator=g)
+    sur.forward(X, keep=True)
+    loss = sur.backward(X, X.T.contiguous(), T, want_dx=True)
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    l_ref, gW, gb, dx = cpu_reference(sur, X, T)
+    assert abs(loss.item() - l_ref.item()) <= 1e-4 * abs(l_ref.item())
+    rel = lambda a, b: ((a.double().cpu() - b).norm() / b.norm()).item()  # noqa: E731
+    for i in range(5):
+        out = sur.W[i].shape[0]
+        assert rel(sur.gW[i][:out], gW[i]) < 3e-3, (i, rel(sur.gW[i][:out], gW[i]))
+        assert rel(sur.gb[i], gb[i]) < 3e-3, (i, rel(sur.gb[i], gb[i]))
+    assert rel(sur.dX(B), dx) < 3e-3
+
+
+def test_adam_matches_update_rule():
+    sur = S.Surrogate(DEV, seed=3)
+    w0 = [w.clone() for w in sur.W]
+    for gw in sur.gW:
+        gw.normal_()
+    for gb in sur.gb:
+        gb.normal_()
+    g0 = [gw[:w.shape[0]].clone() for gw, w in zip(sur.gW, sur.W)]
+    sur.adam(lr=1e-2)
+    torch.cuda.synchronize()
+    for w_new, w_old, g in zip(sur.W, w0, g0):
+        m = 0.1 * g
+        v = 0.001 * g * g
+        ref = w_old - 1e-2 * (m / 0.1) / (torch.sqrt(v / 0.001) + 1e-8)
+        assert torch.allclose(w_new, ref, rtol=1e-5, atol=1e-6)
+    # BF16 copies refreshed
+    assert torch.equal(sur.Wb[0], sur.W[0].to(torch.bfloat16))
+    assert torch.equal(sur.Wt[0], sur.W[0].T.contiguous().to(torch.bfloat16))
+
+
+@pytest.fixture(scope="module")
+def trained():
+    sur = S.Surrogate(DEV, seed=0)
+    F, A = S.generate_transitions(sur, 8192, 60, DEV, seed=0)
+    S.fit_normalisation(sur, F, A)
+    X, T = S.normalise(sur, F[:16384], A[:16384])
+    sur.forward(X, keep=True)
+    l0 = sur.backward(X, X.T.contiguous(), T).item()
+    hist = S.train(sur, F, A, steps=400, batch=16384, lr=1e-3)
+    sur.forward(X, keep=True)
+    l1 = sur.backward(X, X.T.contiguous(), T).item()
+    torch.cuda.synchronize()
+    return sur, l0, l1
+
+
+def test_training_lowers_the_loss(trained):
+    sur, l0, l1 = trained
+    print(f"surrogate loss (normalised qacc MSE): before {l0:.4f}, after 400 steps {l1:.4f}")
+    assert S.gemm_status() == 0
+    assert np.isfinite(l1) and l1 < 0.5 * l0
+
+
+def make_state(n, seed=0):
+    from g1sim_b200 import workloads
+    w = workloads.randomized(nenv=n, seed=seed)
+    s = {k: torch.tensor(w[k], dtype=torch.float32, device=DEV) for k in ("qpos", "qvel", "anchor", "ctrl")}
+    s["contact_forces"] = torch.zeros(8, n, device=DEV)
+    return s
+
+
+def test_fallback_rollout(trained):
+    sur, _, _ = trained
+    n = 1024
+    cfg = _lib.default_config(dt=2e-3)
+    a, b = make_state(n), make_state(n)
+    frac, _ = S.rollout_with_fallback(sur, a, 20, bound=0.0)
+    for _ in range(20):
+        G.step(b["qpos"], b["qvel"], b["anchor"], b["ctrl"], 1, config=cfg, contact_forces=b["contact_forces"])
+    assert frac == 0.0
+    assert torch.equal(a["qpos"], b["qpos"]) and torch.equal(a["qvel"], b["qvel"])
+    c = make_state(n, seed=1)
+    frac, med = S.rollout_with_fallback(sur, c, 50, bound=1e-3)
+    print(f"fallback rollout: {100 * frac:.1f} % of env-steps within 1e-3 of the exact step, median one-step error {med:.2e}")
+    assert torch.isfinite(c["qpos"]).all() and 0.0 <= frac <= 1.0
+
+
+def test_surrogate_gradient_is_smooth_across_touchdown(trained, oracle):
+    """d qacc_z / d z of the exact step (FP64 oracle, central differences)
+    jumps where the lowest foot sphere touches down; the surrogate's
+    derivative (its backward kernels) does not."""
+    sur, _, _ = trained
+    stand = np.asarray(M.qpos_stand, dtype=np.float64)
+    zs = np.linspace(0.745, 0.765, 64)
+    h = 1e-7
+
+    def exact_az(z):
+        q = stand.copy()
+        q[2] = z
+        v = np.zeros(35)
+        an = np.full(16, 1e30)
+        oracle.c_step(q, v, stand[7:].copy(), 1, 2e-3, an)
+        return v[2] / 2e-3
+
+    d_exact = np.array([(exact_az(z + h) - exact_az(z - h)) / (2 * h) for z in zs])
+    # surrogate: d (predicted qacc_z) / d z through the input-gradient kernel
+    n = 128
+    q = torch.tensor(np.repeat(stand[:, None], n, axis=1), dtype=torch.float32, device=DEV)
+    q[2, :64] = torch.tensor(zs, dtype=torch.float32, device=DEV)
+    v = torch.zeros(35, n, device=DEV)
+    ct = q[7:].clone()
+    X = torch.empty(n, 128, dtype=torch.bfloat16, device=DEV)
+    sur.features(q, v, ct, torch.zeros(8, n, device=DEV), X)
+    Y = sur.forward(X, keep=True).clone()
+    w = torch.zeros(64, device=DEV)
+    w[2] = 1.0
+    T = Y.clone()
+    T[:, 2] -= n / 2.0  # d loss / d Y = e_2 for every row
+    sur.backward(X, X.T.contiguous(), T, want_dx=True, weights=w)
+    zi = 58  # feature index of the base height
+    d_sur = (sur.dX(n)[:64, zi] * sur.in_istd[zi] * sur.out_std[2]).double().cpu().numpy()
+    jump_exact = np.abs(np.diff(d_exact)).max()
+    jump_sur = np.abs(np.diff(d_sur)).max()
+    print(f"max step of d qacc_z/dz between z samples: exact {jump_exact:.1f}, surrogate {jump_sur:.2f} (1/s^2)")
+    assert jump_exact > 10.0 * max(jump_sur, 1e-3)
