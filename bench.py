@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--surrogate-steps", type=int, default=300, help="training steps of the surrogate (-1: skip)")
     return p.parse_args()
 
 
@@ -299,6 +300,77 @@ def adjoint_bench(device, stream, steps, warmup, world):
             "finite": bool(torch.isfinite(r["grad_targets"]).all().item())}
 
 
+# ------------------------------------------------------ dynamics surrogate
+SUR_ENVS, SUR_GEN_STEPS, SUR_BATCH = 65536, 153, 65536  # 10.0M transitions
+
+
+def surrogate_bench(device, train_steps, world):
+    """Config of the learned dynamics surrogate: 10.0M transitions of the
+    randomised workload's simulator (65,536 envs x 153 steps), MLP 4 x 512
+    SiLU trained with batch 65,536 on the library's kernels (BF16 tcgen05
+    GEMMs, FP32 accumulation), then a 50-step rollout of 65,536 envs with
+    per-env fallback to the exact step where the one-step error exceeds 1e-3."""
+    import torch
+    from g1sim_b200 import surrogate as S
+    sur = S.Surrogate(device, seed=0)
+    t0 = time.perf_counter()
+    F, A = S.generate_transitions(sur, SUR_ENVS, SUR_GEN_STEPS, device, seed=1)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    S.fit_normalisation(sur, F, A)
+    X, T = S.normalise(sur, F, A)
+    del F
+    g = torch.Generator(device=device).manual_seed(0)
+    idx = torch.randint(0, X.shape[0], (SUR_BATCH,), generator=g, device=device)
+    xb, tb = X[idx].contiguous(), T[idx].contiguous()
+    xt = xb.T.contiguous()
+    sur.forward(xb, keep=True)
+    l0 = float(sur.backward(xb, xt, tb).item())
+    # timed training steps (the same minibatch each step keeps the timed region to the kernels)
+    for _ in range(3):
+        sur.train_step(xb, xt, tb, lr=1e-3)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        sur.train_step(xb, xt, tb, lr=1e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / 10
+    macs = sum(S.DIMS[i] * S.DIMS[i + 1] for i in range(5))
+    train_tflops = 3 * 2 * SUR_BATCH * macs / (step_ms * 1e-3) / 1e12
+    # inference throughput of the network alone (features in HBM)
+    e0.record()
+    for _ in range(10):
+        sur.forward(xb)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / 10
+    # the rest of the training budget on random minibatches
+    hist = []
+    for k in range(train_steps):
+        idx = torch.randint(0, X.shape[0], (SUR_BATCH,), generator=g, device=device)
+        xb = X[idx].contiguous()
+        lr = 1e-3 * (0.1 ** (k / max(train_steps, 1)))
+        hist.append(sur.train_step(xb, xb.T.contiguous(), T[idx].contiguous(), lr=lr))
+    torch.cuda.synchronize()
+    l1 = float(hist[-1].item()) if hist else l0
+    from g1sim_b200 import workloads
+    w = workloads.randomized(nenv=SUR_ENVS, seed=7)
+    st = {k: torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("qpos", "qvel", "anchor", "ctrl")}
+    st["contact_forces"] = torch.zeros(8, SUR_ENVS, device=device)
+    frac, med = S.rollout_with_fallback(sur, st, 50, bound=1e-3)
+    return {"train_step_ms": step_ms, "train_tflops": train_tflops,
+            "train_flops_per_step": 3 * 2 * SUR_BATCH * macs,
+            "inference": {"value": SUR_BATCH / (fwd_ms * 1e-3), "unit": "env-steps/s (network forward only)"},
+            "transitions": int(X.shape[0]), "generation_s": gen_s, "train_steps": train_steps,
+            "loss_start": l0, "loss_end": l1,
+            "fallback_rollout": {"envs": SUR_ENVS, "steps": 50, "bound": 1e-3,
+                                 "fraction_surrogate": frac, "median_one_step_error": med},
+            "gemm_status": S.gemm_status()}
+
+
 # ------------------------------------------------------------- our arm
 def ours(args, world, rank, local):
     import torch
@@ -426,6 +498,7 @@ def ours(args, world, rank, local):
 
     pol = policy_fused_bench(n, rank, device, stream, args.steps, args.warmup, world, local, init)
     adj = adjoint_bench(device, stream, args.steps, args.warmup, world) if not args.no_adjoint else None
+    sur = surrogate_bench(device, args.surrogate_steps, world) if args.surrogate_steps >= 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -454,6 +527,8 @@ def ours(args, world, rank, local):
         }
         if adj is not None:
             line["adjoint"] = adj
+        if sur is not None:
+            line["surrogate"] = sur
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))
