@@ -1042,14 +1042,15 @@ static int launched(const char* what) {
 
 int g1b_sur_act(int B, int D, const float* Z, void* H, void* Ht, void* stream) {
   if (B <= 0 || D <= 0 || !Z || !H) return fail("sur_act: invalid arguments");
-  sur_act_kernel<<<grid_1d((size_t)B * D, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+  const dim3 grid((D + 31) / 32, (B + 31) / 32), block(32, 8);
+  sur_act_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       B, D, Z, static_cast<__nv_bfloat16*>(H), static_cast<__nv_bfloat16*>(Ht));
   return launched("sur_act_kernel");
 }
 
 int g1b_sur_act_bwd(int B, int D, const float* dH, const float* Z, void* dZ, void* dZt, float* db, void* stream) {
   if (B <= 0 || D <= 0 || !dH || !Z || !dZ || !dZt || !db) return fail("sur_act_bwd: invalid arguments");
-  const dim3 grid((D + 31) / 32, 128), block(32, 8);
+  const dim3 grid((D + 31) / 32, (B + 31) / 32), block(32, 8);
   sur_act_bwd_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       B, D, dH, Z, static_cast<__nv_bfloat16*>(dZ), static_cast<__nv_bfloat16*>(dZt), db);
   return launched("sur_act_bwd_kernel");
@@ -1058,7 +1059,7 @@ int g1b_sur_act_bwd(int B, int D, const float* dH, const float* Z, void* dZ, voi
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream) {
   if (B <= 0 || D <= 0 || !Y || !T || !w || !dY || !dYt || !db || !loss) return fail("sur_loss: invalid arguments");
-  const dim3 grid((D + 31) / 32, 128), block(32, 8);
+  const dim3 grid((D + 31) / 32, (B + 31) / 32), block(32, 8);
   sur_loss_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       B, D, Y, T, w, static_cast<__nv_bfloat16*>(dY), static_cast<__nv_bfloat16*>(dYt), db, loss);
   return launched("sur_loss_kernel");

@@ -19,41 +19,60 @@ __device__ __forceinline__ float silu_grad(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
+// The element-wise kernels below work on 32 x 32 tiles (block 32 x 8): rows
+// r0..r0+31 of the batch and columns c0..c0+31, reading and writing the
+// row-major arrays along columns and the transposed copies along rows
+// through a shared-memory tile, so both sides are coalesced.
+
 // H = SiLU(Z) (BF16, [B][D]) and its transpose Ht ([D][B], nullable).
 __global__ void sur_act_kernel(int B, int D, const float* __restrict__ Z, __nv_bfloat16* H, __nv_bfloat16* Ht) {
-  const size_t total = (size_t)B * D;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(i / D), c = (int)(i % D);
-    const __nv_bfloat16 h = __float2bfloat16_rn(silu(Z[i]));
-    H[i] = h;
-    if (Ht) Ht[(size_t)c * B + r] = h;
+  __shared__ __nv_bfloat16 t[32][34];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < B && c < D) {
+      const size_t i = (size_t)r * D + c;
+      const __nv_bfloat16 h = __float2bfloat16_rn(silu(Z[i]));
+      H[i] = h;
+      t[k][threadIdx.x] = h;
+    }
+  }
+  if (!Ht) return;
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < B && c < D) Ht[(size_t)c * B + r] = t[threadIdx.x][k];
   }
 }
 
-// dZ = dH * SiLU'(Z): BF16 [B][D] and transposed [D][B] (rows D..Dt of the
-// transpose are left as the caller zeroed them); db[c] += sum_r dZ[r][c].
-// Block (32, 8): 32 columns x 8 row-groups; rows strided.
+// dZ = dH * SiLU'(Z): BF16 [B][D] and transposed [D][B]; db[c] += column sums.
 __global__ void sur_act_bwd_kernel(int B, int D, const float* __restrict__ dH, const float* __restrict__ Z,
                                    __nv_bfloat16* dZ, __nv_bfloat16* dZt, float* db) {
-  const int c = blockIdx.x * 32 + threadIdx.x;
+  __shared__ __nv_bfloat16 t[32][34];
+  __shared__ float red[8][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
   float acc = 0.0f;
-  if (c < D) {
-    for (int r = blockIdx.y * 8 + threadIdx.y; r < B; r += gridDim.y * 8) {
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < B && c < D) {
       const size_t i = (size_t)r * D + c;
       const float g = dH[i] * silu_grad(Z[i]);
       acc += g;
       const __nv_bfloat16 gb = __float2bfloat16_rn(g);
       dZ[i] = gb;
-      dZt[(size_t)c * B + r] = gb;
+      t[k][threadIdx.x] = gb;
     }
   }
-  __shared__ float red[8][33];
   red[threadIdx.y][threadIdx.x] = acc;
   __syncthreads();
-  if (threadIdx.y == 0 && c < D) {
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < B && c < D) dZt[(size_t)c * B + r] = t[threadIdx.x][k];
+  }
+  if (threadIdx.y == 0 && c0 + threadIdx.x < D) {
     float s = 0.0f;
     for (int k = 0; k < 8; ++k) s += red[k][threadIdx.x];
-    atomicAdd(db + c, s);
+    atomicAdd(db + c0 + threadIdx.x, s);
   }
 }
 
@@ -62,11 +81,15 @@ __global__ void sur_act_bwd_kernel(int B, int D, const float* __restrict__ dH, c
 __global__ void sur_loss_kernel(int B, int D, const float* __restrict__ Y, const float* __restrict__ T,
                                 const float* __restrict__ w, __nv_bfloat16* dY, __nv_bfloat16* dYt, float* db,
                                 float* loss) {
-  const int c = blockIdx.x * 32 + threadIdx.x;
+  __shared__ __nv_bfloat16 t[32][34];
+  __shared__ float red[2][8][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const int c = c0 + threadIdx.x;
+  const float wc = c < D ? w[c] : 0.0f;
   float acc = 0.0f, l = 0.0f;
-  if (c < D) {
-    const float wc = w[c];
-    for (int r = blockIdx.y * 8 + threadIdx.y; r < B; r += gridDim.y * 8) {
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int r = r0 + k;
+    if (r < B && c < D) {
       const size_t i = (size_t)r * D + c;
       const float e = Y[i] - T[i];
       l += wc * e * e;
@@ -74,13 +97,16 @@ __global__ void sur_loss_kernel(int B, int D, const float* __restrict__ Y, const
       acc += g;
       const __nv_bfloat16 gb = __float2bfloat16_rn(g);
       dY[i] = gb;
-      dYt[(size_t)c * B + r] = gb;
+      t[k][threadIdx.x] = gb;
     }
   }
-  __shared__ float red[2][8][33];
   red[0][threadIdx.y][threadIdx.x] = acc;
   red[1][threadIdx.y][threadIdx.x] = l;
   __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int cc = c0 + k, r = r0 + threadIdx.x;
+    if (r < B && cc < D) dYt[(size_t)cc * B + r] = t[threadIdx.x][k];
+  }
   if (threadIdx.y == 0 && c < D) {
     float s = 0.0f, ls = 0.0f;
     for (int k = 0; k < 8; ++k) {
