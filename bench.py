@@ -41,6 +41,11 @@ FLOPS_PER_ENV_STEP = 36600.0
 # anchor 16, ctrl 29, mu, dmass) and out (qpos, qvel, anchor, ctrl), float32.
 BYTES_PER_ENV_LAUNCH = 4.0 * ((36 + 35 + 16 + 29 + 2) + (36 + 35 + 16 + 29))
 
+# DRAM bytes per env of one split_kernel launch (10 substeps), from one ncu
+# capture at 16,384 envs (dram__bytes_read.sum + dram__bytes_write.sum =
+# 6,105,088 + 0 B; profiles/split_kernel_16384env_full.md), scaled by envs.
+NCU_DRAM_BYTES_PER_ENV_LAUNCH = 6105088.0 / 16384
+
 NENV = 65536
 SUBSTEPS = 1000
 DECIM = 10
@@ -514,7 +519,10 @@ def ours(args, world, rank, local):
                        "envs_per_gpu": n, "substeps": SUBSTEPS, "decimation": DECIM, "dt": DT,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
             "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
-                         "frac": achieved_tf / peak_tf if peak_tf > 0 else None, "traffic": None,
+                         "frac": achieved_tf / peak_tf if peak_tf > 0 else None,
+                         "traffic": NCU_DRAM_BYTES_PER_ENV_LAUNCH * n,
+                         "traffic_source": "ncu DRAM bytes of one split_kernel launch at 16,384 envs, scaled by envs",
+                         "algorithmic_bytes": BYTES_PER_ENV_LAUNCH * n,
                          "peak_source": "measured FFMA microbenchmark (g1b_ffma_peak), this run",
                          "flops_per_env_step": FLOPS_PER_ENV_STEP, "kernel": kernel_name,
                          "kernel_ms": launch_ms, "hbm_gbs": hbm_gbs},

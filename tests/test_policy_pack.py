@@ -145,3 +145,18 @@ def test_gae_matches_reference_recursion():
             last = delta + 0.99 * 0.95 * nnt * last
             assert abs(float(adv[t, e]) - last) < 1e-5
             assert abs(float(ret[t, e]) - (last + float(v[t, e]))) < 1e-5
+
+
+def test_policy_pt_round_trip(tmp_path):
+    ac = P.ActorCritic().xavier_(torch.Generator().manual_seed(4))
+    with torch.no_grad():
+        ac.obs_mean.uniform_(-1, 1)
+        ac.std.fill_(-0.7)
+    path = tmp_path / "policy.pt"
+    torch.save(ac.state_dict(), path)
+    bc = P.load_policy_pt(str(path), device="cpu")
+    for (ka, va), (kb, vb) in zip(ac.state_dict().items(), bc.state_dict().items()):
+        assert ka == kb and torch.equal(va, vb)
+    wa, ba = P.pack_weights(ac)
+    wb, bb = P.pack_weights(bc)
+    assert torch.equal(wa, wb) and torch.equal(ba, bb)
