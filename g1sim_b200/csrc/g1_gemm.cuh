@@ -6,7 +6,7 @@
 // ldb in elements); C is FP32 row-major (ldc).  One CTA (128 threads) owns
 // a 128 x Nt tile of C (Nt = min(N, 256), an MMA's N) and a K range of its
 // split: 64-wide K chunks are copied global -> shared with 16-byte cp.async
-// into the UMMA no-swizzle K-major layout (two stages), thread 0 issues
+// into the UMMA 128-byte-swizzle K-major layout (kGemmStages-deep ring), thread 0 issues
 // tcgen05.mma (M 128, K 16) into a tensor-memory accumulator, and the four
 // warps read their 32 lanes back for the epilogue.  With several K splits
 // the partial tiles are added into C with atomics (C zeroed by the caller).
@@ -19,7 +19,8 @@ constexpr int kGemmMaxN = 256;
 constexpr uint32_t kGemmABytes = 128 * kGemmKC * 2;        // 16 KB
 constexpr uint32_t kGemmBBytes = kGemmMaxN * kGemmKC * 2;  // 32 KB
 constexpr uint32_t kGemmStage = kGemmABytes + kGemmBBytes;
-constexpr size_t kGemmSmem = 2 * (size_t)kGemmStage;
+constexpr int kGemmStages = 4;  // chunks in flight: 3 copying while one is multiplied
+constexpr size_t kGemmSmem = kGemmStages * (size_t)kGemmStage + 1024;  // + alignment slack
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
@@ -31,16 +32,26 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Copy K chunk [k0, k0 + 64) of rows [r0, r0 + rows) of a row-major BF16
-// matrix into a [8][rows/8][8][8] tile at shared address dst.
+// matrix into shared memory at dst (1024-byte aligned) in the UMMA K-major
+// 128-byte-swizzle layout: each row's 64 values are one 128-byte line, eight
+// lines form a 1024-byte atom, and the 16-byte piece j of row r sits at piece
+// position j ^ (r % 8) of its line (bank-conflict-free for the tensor core).
 __device__ __forceinline__ void gemm_load_tile(uint32_t dst, const __nv_bfloat16* X, int ld, int r0, int rows,
                                                int k0) {
   const int pieces = rows * (kGemmKC / 8);
   for (int p = threadIdx.x; p < pieces; p += 128) {
-    const int r = p >> 3, k8 = (p & 7) * 8;
-    const __nv_bfloat16* src = X + (size_t)(r0 + r) * ld + k0 + k8;
-    const uint32_t off = (uint32_t)((k8 >> 3) * (rows >> 3) + (r >> 3)) * 128u + (uint32_t)(r & 7) * 16u;
+    const int r = p >> 3, j = p & 7;
+    const __nv_bfloat16* src = X + (size_t)(r0 + r) * ld + k0 + j * 8;
+    const uint32_t off = (uint32_t)(r >> 3) * 1024u + (uint32_t)(r & 7) * 128u + (uint32_t)((j ^ (r & 7)) * 16);
     cp_async16(dst + off, src);
   }
+}
+// Shared-memory descriptor of such a tile, K step kk (16 values = 32 bytes
+// along the line): swizzle mode 128B (2), stride between 8-row atoms 1024 B.
+__device__ __forceinline__ uint64_t gemm_desc_sw128(uint32_t tile, int kk) {
+  const uint32_t a = tile + (uint32_t)kk * 32u;
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
 }
 
 template <bool kAtomic>
@@ -48,17 +59,15 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
                                                         const __nv_bfloat16* __restrict__ B, int ldb, float* C,
                                                         int ldc, const float* __restrict__ bias, int Nt, int Ks,
                                                         int* err) {
-  extern __shared__ __align__(128) uint8_t gsm[];
-  __shared__ uint64_t bars[3];  // mma done per stage, accumulator
+  extern __shared__ __align__(1024) uint8_t gsm[];
+  __shared__ uint64_t bars[kGemmStages + 1];  // mma done per stage, accumulator
   __shared__ uint32_t tslot;
   const int m0 = blockIdx.x * 128, n0 = blockIdx.y * Nt, kbeg = blockIdx.z * Ks;
   const int nchunks = Ks / kGemmKC;
-  const uint32_t sbase = tc::smem_u32(gsm);
-  const uint32_t bar0 = tc::smem_u32(&bars[0]), bar1 = tc::smem_u32(&bars[1]), bacc = tc::smem_u32(&bars[2]);
+  const uint32_t sbase = (tc::smem_u32(gsm) + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
+  const uint32_t bacc = tc::smem_u32(&bars[kGemmStages]);
   if (threadIdx.x == 0) {
-    tc::mbar_init(bar0, 1);
-    tc::mbar_init(bar1, 1);
-    tc::mbar_init(bacc, 1);
+    for (int i = 0; i <= kGemmStages; ++i) tc::mbar_init(tc::smem_u32(&bars[i]), 1);
     tc::mbar_fence_init();
   }
   if (threadIdx.x < 32) {
@@ -72,40 +81,42 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   tc::tc_fence_after();
   const uint32_t tmem = tslot;
   const uint32_t idesc = tc::idesc_bf16(128, Nt);
-  const uint32_t lbo_a = 128 * 16, lbo_b = (uint32_t)Nt * 16;
   bool ok = true;
 
-  gemm_load_tile(sbase, A, lda, m0, 128, kbeg);
-  gemm_load_tile(sbase + kGemmABytes, B, ldb, n0, Nt, kbeg);
-  cp_async_commit();
-  for (int c = 0; c < nchunks; ++c) {
-    const int s = c & 1;
-    if (c + 1 < nchunks) {
-      const int s1 = (c + 1) & 1;
-      // the stage was last read by the MMAs of chunk c - 1
-      if (c >= 1 && !tc::mbar_wait(s1 ? bar1 : bar0, ((c - 1) >> 1) & 1)) ok = false;
-      const uint32_t st = sbase + (uint32_t)s1 * kGemmStage;
-      gemm_load_tile(st, A, lda, m0, 128, kbeg + (c + 1) * kGemmKC);
-      gemm_load_tile(st + kGemmABytes, B, ldb, n0, Nt, kbeg + (c + 1) * kGemmKC);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  // prologue: chunks 0 .. kGemmStages - 2 (one commit group each, empty groups past the end)
+  for (int i = 0; i < kGemmStages - 1; ++i) {
+    if (i < nchunks) {
+      const uint32_t st = sbase + (uint32_t)i * kGemmStage;
+      gemm_load_tile(st, A, lda, m0, 128, kbeg + i * kGemmKC);
+      gemm_load_tile(st + kGemmABytes, B, ldb, n0, Nt, kbeg + i * kGemmKC);
     }
+    cp_async_commit();
+  }
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c % kGemmStages;
+    cp_async_wait<kGemmStages - 2>();  // this thread's copies of chunk c have landed
     tc::fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
       tc::tc_fence_after();
       const uint32_t st = sbase + (uint32_t)s * kGemmStage;
 #pragma unroll
-      for (int j = 0; j < kGemmKC / 16; ++j) {
-        const uint64_t ad = tc::sdesc(st + (uint32_t)j * 2 * lbo_a, lbo_a, 128);
-        const uint64_t bd = tc::sdesc(st + kGemmABytes + (uint32_t)j * 2 * lbo_b, lbo_b, 128);
-        tc::mma_bf16(tmem, ad, bd, idesc, (c > 0 || j > 0) ? 1u : 0u);
-      }
-      tc::mma_commit(s ? bar1 : bar0);
+      for (int j = 0; j < kGemmKC / 16; ++j)
+        tc::mma_bf16(tmem, gemm_desc_sw128(st, j), gemm_desc_sw128(st + kGemmABytes, j), idesc,
+                     (c > 0 || j > 0) ? 1u : 0u);
+      tc::mma_commit(tc::smem_u32(&bars[s]));
       if (c + 1 == nchunks) tc::mma_commit(bacc);
     }
+    // refill the stage read by chunk c - 1 with chunk c + kGemmStages - 1
+    const int nx = c + kGemmStages - 1;
+    if (nx < nchunks) {
+      const int sp = nx % kGemmStages;
+      if (c >= 1 && !tc::mbar_wait(tc::smem_u32(&bars[sp]), ((c - 1) / kGemmStages) & 1)) ok = false;
+      const uint32_t st = sbase + (uint32_t)sp * kGemmStage;
+      gemm_load_tile(st, A, lda, m0, 128, kbeg + nx * kGemmKC);
+      gemm_load_tile(st + kGemmABytes, B, ldb, n0, Nt, kbeg + nx * kGemmKC);
+    }
+    cp_async_commit();
   }
   if (!tc::mbar_wait(bacc, 0)) ok = false;
   tc::tc_fence_after();

@@ -107,14 +107,16 @@ __global__ void sur_loss_kernel(int B, int D, const float* __restrict__ Y, const
     const int cc = c0 + k, r = r0 + threadIdx.x;
     if (r < B && cc < D) dYt[(size_t)cc * B + r] = t[threadIdx.x][k];
   }
-  if (threadIdx.y == 0 && c < D) {
+  if (threadIdx.y == 0) {
     float s = 0.0f, ls = 0.0f;
     for (int k = 0; k < 8; ++k) {
       s += red[0][k][threadIdx.x];
       ls += red[1][k][threadIdx.x];
     }
-    atomicAdd(db + c, s);
-    atomicAdd(loss, ls / (float)B);
+    if (c < D) atomicAdd(db + c, s);
+    // one loss atomic per block (warp sum), not one per column
+    for (int o = 16; o > 0; o >>= 1) ls += __shfl_xor_sync(0xffffffffu, ls, o);
+    if (threadIdx.x == 0) atomicAdd(loss, ls / (float)B);
   }
 }
 
