@@ -240,6 +240,34 @@ int g1b_adjoint_noalloc(int nenv, const g1b_config* cfg, const g1b_adjoint_probl
                         const float* kd_scale, float* loss, float* grad_targets, float* grad_kp, float* grad_kd,
                         float* grad_qpos0, float* grad_qvel0, void* stream);
 
+/* ------------------------------------------------- dynamics surrogate */
+/* No reference counterpart (the learned surrogate of the workload
+ * configuration).  BF16 tcgen05 GEMM, FP32 accumulation:
+ *   C[M x N] = A[M x K] . B[N x K]^T (+ bias[N]), A, B row-major with K
+ *   contiguous; splits > 1 splits K over CTAs and adds into C atomically
+ *   (C cleared first).  M % 128 == 0, N % 16 == 0 (N % 256 == 0 above 256),
+ *   K % (64 splits) == 0, lda / ldb multiples of 8, ldc of 4. */
+int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                  const float* bias, int splits, void* stream);
+/* Device status of the GEMM kernels since the last call (synchronises):
+ * 0 ok, 1 a pipeline wait timed out.  Clears the flag. */
+int g1b_gemm_status(int* code);
+/* Element-wise kernels of the surrogate: SiLU with transposed copy, its
+ * backward with bias-gradient sums, weighted MSE and its gradient, Adam,
+ * BF16 weight copies, the feature vector of the state, and the
+ * surrogate's state update (qacc -> qvel, qpos). */
+int g1b_sur_act(int B, int D, const float* Z, void* H, void* Ht, void* stream);
+int g1b_sur_act_bwd(int B, int D, const float* dH, const float* Z, void* dZ, void* dZt, float* db, void* stream);
+int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
+                 float* loss, void* stream);
+int g1b_sur_adam(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
+                 int step, void* stream);
+int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* stream);
+int g1b_sur_features(int n, const float* qpos, const float* qvel, const float* ctrl, const float* cf,
+                     const float* mean, const float* istd, void* X, void* Xt, float* F, void* stream);
+int g1b_sur_integrate(int n, const float* Y, int ldy, const float* omean, const float* ostd, float dt, float* qpos,
+                      float* qvel, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
