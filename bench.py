@@ -305,6 +305,14 @@ def adjoint_bench(device, stream, steps, warmup, world):
             "finite": bool(torch.isfinite(r["grad_targets"]).all().item())}
 
 
+def measured_bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 # ------------------------------------------------------ dynamics surrogate
 SUR_ENVS, SUR_GEN_STEPS, SUR_BATCH = 65536, 153, 65536  # 10.0M transitions
 
@@ -366,7 +374,10 @@ def surrogate_bench(device, train_steps, world):
     st = {k: torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("qpos", "qvel", "anchor", "ctrl")}
     st["contact_forces"] = torch.zeros(8, SUR_ENVS, device=device)
     frac, med = S.rollout_with_fallback(sur, st, 50, bound=1e-3)
+    peak = measured_bf16_peak()
     return {"train_step_ms": step_ms, "train_tflops": train_tflops,
+            "train_frac_of_bf16_peak": (train_tflops / peak) if peak else None,
+            "bf16_peak_tflops": peak, "bf16_peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured",
             "train_flops_per_step": 3 * 2 * SUR_BATCH * macs,
             "inference": {"value": SUR_BATCH / (fwd_ms * 1e-3), "unit": "env-steps/s (network forward only)"},
             "transitions": int(X.shape[0]), "generation_s": gen_s, "train_steps": train_steps,

@@ -30,7 +30,6 @@ pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda", 0)
 H, NENV = 64, 16
 STAND = np.asarray(M.qpos_stand)
-RANGE = np.asarray(M.jnt_range)
 
 
 def problem(golden_host, n=NENV, seed=0):

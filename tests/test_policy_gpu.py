@@ -19,8 +19,6 @@ Checks, each against an independent restatement:
     bit; timers and command redraws within their ranges;
   * one launch of 8 policy steps equals 8 launches of one, bit for bit.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
 import torch
