@@ -373,7 +373,7 @@ def surrogate_bench(device, train_steps, world):
     w = workloads.randomized(nenv=SUR_ENVS, seed=7)
     st = {k: torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("qpos", "qvel", "anchor", "ctrl")}
     st["contact_forces"] = torch.zeros(8, SUR_ENVS, device=device)
-    frac, med = S.rollout_with_fallback(sur, st, 50, bound=1e-3)
+    frac, err = S.rollout_with_fallback(sur, st, 50, bound=1e-3)
     peak = measured_bf16_peak()
     return {"train_step_ms": step_ms, "train_tflops": train_tflops,
             "train_frac_of_bf16_peak": (train_tflops / peak) if peak else None,
@@ -383,7 +383,7 @@ def surrogate_bench(device, train_steps, world):
             "transitions": int(X.shape[0]), "generation_s": gen_s, "train_steps": train_steps,
             "loss_start": l0, "loss_end": l1,
             "fallback_rollout": {"envs": SUR_ENVS, "steps": 50, "bound": 1e-3,
-                                 "fraction_surrogate": frac, "median_one_step_error": med},
+                                 "fraction_surrogate": frac, "one_step_error": err},
             "gemm_status": S.gemm_status()}
 
 

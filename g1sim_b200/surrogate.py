@@ -291,7 +291,8 @@ def rollout_with_fallback(sur, s, steps, dt=2e-3, bound=1e-3, mu=None, dmass=Non
     """Advance every env `steps` steps: with the surrogate where its one-step
     error against the exact step is <= bound (relative per component of
     qpos and qvel), else with the exact step.  Returns (fraction of env-steps
-    taken by the surrogate, median one-step error)."""
+    taken by the surrogate, statistics of the one-step error: median, 90th
+    percentile and the fractions of env-steps within 1e-2 and 1e-1)."""
     cfg = _lib.default_config(dt=dt)
     used, errs = 0, []
     n = s["qpos"].shape[1]
@@ -310,4 +311,7 @@ def rollout_with_fallback(sur, s, steps, dt=2e-3, bound=1e-3, mu=None, dmass=Non
         s["qvel"].copy_(torch.where(ok[None], vs, ex["qvel"]))
         s["anchor"].copy_(ex["anchor"])
     e = torch.cat(errs)
-    return used / float(n * steps), float(e.median().item())
+    stats = {"median": float(e.median().item()), "p90": float(torch.quantile(e[:1 << 24].float(), 0.9).item()),
+             "within_1e-2": float((e <= 1e-2).float().mean().item()),
+             "within_1e-1": float((e <= 1e-1).float().mean().item())}
+    return used / float(n * steps), stats
