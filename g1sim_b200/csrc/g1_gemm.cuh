@@ -4,7 +4,7 @@
 //   C[M x N] (= or +=) A[M x K] . B[N x K]^T (+ bias[N])
 // A and B are BF16, row-major with K contiguous (leading dimensions lda,
 // ldb in elements); C is FP32 row-major (ldc).  One CTA (128 threads) owns
-// a 128 x Nt tile of C (Nt = min(N, 256), an MMA's N) and a K range of its
+// a 128 MT x Nt tile of C (MT = 1 or 2 row tiles, Nt = min(N, 256), an MMA's N) and a K range of its
 // split: 64-wide K chunks are copied global -> shared with 16-byte cp.async
 // into the UMMA 128-byte-swizzle K-major layout (kGemmStages-deep ring), thread 0 issues
 // tcgen05.mma (M 128, K 16) into a tensor-memory accumulator, and the four
@@ -18,9 +18,16 @@ constexpr int kGemmKC = 64;  // K columns per chunk
 constexpr int kGemmMaxN = 256;
 constexpr uint32_t kGemmABytes = 128 * kGemmKC * 2;        // 16 KB
 constexpr uint32_t kGemmBBytes = kGemmMaxN * kGemmKC * 2;  // 32 KB
-constexpr uint32_t kGemmStage = kGemmABytes + kGemmBBytes;
-constexpr int kGemmStages = 4;  // chunks in flight: 3 copying while one is multiplied
-constexpr size_t kGemmSmem = kGemmStages * (size_t)kGemmStage + 1024;  // + alignment slack
+// MT row tiles of 128 per CTA share each B chunk (MT = 2 halves the weight
+// traffic per row, the bound of this kernel); the ring holds 192 KB.
+template <int MT>
+__host__ __device__ constexpr uint32_t gemm_stage_bytes() { return MT * kGemmABytes + kGemmBBytes; }
+template <int MT>
+__host__ __device__ constexpr int gemm_stages() { return MT == 2 ? 3 : 4; }
+template <int MT>
+__host__ __device__ constexpr size_t gemm_smem() {
+  return gemm_stages<MT>() * (size_t)gemm_stage_bytes<MT>() + 1024;  // + alignment slack
+}
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
@@ -54,15 +61,19 @@ __device__ __forceinline__ uint64_t gemm_desc_sw128(uint32_t tile, int kk) {
          (2ull << 61);
 }
 
-template <bool kAtomic>
+template <bool kAtomic, int MT>
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
                                                         const __nv_bfloat16* __restrict__ B, int ldb, float* C,
                                                         int ldc, const float* __restrict__ bias, int Nt, int Ks,
                                                         int* err) {
+  constexpr int kGemmStages = gemm_stages<MT>();
+  constexpr uint32_t kGemmStage = gemm_stage_bytes<MT>();
+  constexpr uint32_t kBOff = MT * kGemmABytes;
+  constexpr uint32_t kCols = 256 * MT;
   extern __shared__ __align__(1024) uint8_t gsm[];
   __shared__ uint64_t bars[kGemmStages + 1];  // mma done per stage, accumulator
   __shared__ uint32_t tslot;
-  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * Nt, kbeg = blockIdx.z * Ks;
+  const int m0 = blockIdx.x * 128 * MT, n0 = blockIdx.y * Nt, kbeg = blockIdx.z * Ks;
   const int nchunks = Ks / kGemmKC;
   const uint32_t sbase = (tc::smem_u32(gsm) + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
   const uint32_t bacc = tc::smem_u32(&bars[kGemmStages]);
@@ -72,7 +83,7 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   }
   if (threadIdx.x < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tslot)),
-                 "r"(256)
+                 "r"(kCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -87,8 +98,8 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   for (int i = 0; i < kGemmStages - 1; ++i) {
     if (i < nchunks) {
       const uint32_t st = sbase + (uint32_t)i * kGemmStage;
-      gemm_load_tile(st, A, lda, m0, 128, kbeg + i * kGemmKC);
-      gemm_load_tile(st + kGemmABytes, B, ldb, n0, Nt, kbeg + i * kGemmKC);
+      gemm_load_tile(st, A, lda, m0, 128 * MT, kbeg + i * kGemmKC);
+      gemm_load_tile(st + kBOff, B, ldb, n0, Nt, kbeg + i * kGemmKC);
     }
     cp_async_commit();
   }
@@ -102,8 +113,10 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
       const uint32_t st = sbase + (uint32_t)s * kGemmStage;
 #pragma unroll
       for (int j = 0; j < kGemmKC / 16; ++j)
-        tc::mma_bf16(tmem, gemm_desc_sw128(st, j), gemm_desc_sw128(st + kGemmABytes, j), idesc,
-                     (c > 0 || j > 0) ? 1u : 0u);
+#pragma unroll
+        for (int t = 0; t < MT; ++t)
+          tc::mma_bf16(tmem + (uint32_t)(t * 256), gemm_desc_sw128(st + (uint32_t)t * kGemmABytes, j),
+                       gemm_desc_sw128(st + kBOff, j), idesc, (c > 0 || j > 0) ? 1u : 0u);
       tc::mma_commit(tc::smem_u32(&bars[s]));
       if (c + 1 == nchunks) tc::mma_commit(bacc);
     }
@@ -113,37 +126,40 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
       const int sp = nx % kGemmStages;
       if (c >= 1 && !tc::mbar_wait(tc::smem_u32(&bars[sp]), ((c - 1) / kGemmStages) & 1)) ok = false;
       const uint32_t st = sbase + (uint32_t)sp * kGemmStage;
-      gemm_load_tile(st, A, lda, m0, 128, kbeg + nx * kGemmKC);
-      gemm_load_tile(st + kGemmABytes, B, ldb, n0, Nt, kbeg + nx * kGemmKC);
+      gemm_load_tile(st, A, lda, m0, 128 * MT, kbeg + nx * kGemmKC);
+      gemm_load_tile(st + kBOff, B, ldb, n0, Nt, kbeg + nx * kGemmKC);
     }
     cp_async_commit();
   }
   if (!tc::mbar_wait(bacc, 0)) ok = false;
   tc::tc_fence_after();
-  // epilogue: warp w holds rows 32 w .. 32 w + 31 of the tile
-  const int row = m0 + (int)threadIdx.x;
-  const uint32_t lane_base = tmem + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
-  float* crow = C + (size_t)row * ldc + n0;
-  for (int c = 0; c < Nt; c += 32) {
-    float v[32];
-    tc::tmem_ld32(lane_base + (uint32_t)c, v);
-    if (bias && blockIdx.z == 0) {
+  // epilogue: warp w holds rows 32 w .. 32 w + 31 of each 128-row subtile
+  for (int t = 0; t < MT; ++t) {
+    const int row = m0 + t * 128 + (int)threadIdx.x;
+    const uint32_t lane_base = tmem + (uint32_t)(t * 256) + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
+    float* crow = C + (size_t)row * ldc + n0;
+    for (int c = 0; c < Nt; c += 32) {
+      float v[32];
+      tc::tmem_ld32(lane_base + (uint32_t)c, v);
+      if (bias && blockIdx.z == 0) {
 #pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] += __ldg(bias + n0 + c + i);
-    }
-    if (c + 32 > Nt) {  // Nt = 16 or 48 ...: partial last group
-      for (int i = 0; i < Nt - c; ++i) {
-        if (kAtomic)
-          atomicAdd(crow + c + i, v[i]);
-        else
-          crow[c + i] = v[i];
+        for (int i = 0; i < 32; ++i) v[i] += __ldg(bias + n0 + c + i);
       }
-    } else if (kAtomic) {
+      if (c + 32 > Nt) {  // Nt = 16 or 48 ...: partial last group
+        for (int i = 0; i < Nt - c; ++i) {
+          if (kAtomic)
+            atomicAdd(crow + c + i, v[i]);
+          else
+            crow[c + i] = v[i];
+        }
+      } else if (kAtomic) {
 #pragma unroll
-      for (int i = 0; i < 32; ++i) atomicAdd(crow + c + i, v[i]);
-    } else {
+        for (int i = 0; i < 32; ++i) atomicAdd(crow + c + i, v[i]);
+      } else {
 #pragma unroll
-      for (int i = 0; i < 32; i += 4) *reinterpret_cast<float4*>(crow + c + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        for (int i = 0; i < 32; i += 4)
+          *reinterpret_cast<float4*>(crow + c + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      }
     }
   }
   if (!ok) atomicExch(err, 1);
@@ -151,5 +167,5 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   __syncthreads();
   tc::tc_fence_after();
   if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
 }

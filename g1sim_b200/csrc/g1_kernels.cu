@@ -997,25 +997,30 @@ int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
   if (lda % 8 || ldb % 8 || ldc % 4 || (((uintptr_t)A | (uintptr_t)B) & 15) || (((uintptr_t)C) & 15))
     return fail("gemm_bf16: lda, ldb multiples of 8, ldc of 4, 16-byte aligned pointers");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const dim3 grid(M / 128, N / Nt, splits);
+  const int MT = M % 256 == 0 ? 2 : 1;  // two row tiles per CTA share each weight chunk
+  const dim3 grid(M / (128 * MT), N / Nt, splits);
   int* err = nullptr;
   cudaError_t e = cudaGetSymbolAddress((void**)&err, g_gemm_error);
   if (e != cudaSuccess) return cuda_fail(e, "gemm_bf16: error flag");
+  const __nv_bfloat16* a = static_cast<const __nv_bfloat16*>(A);
+  const __nv_bfloat16* b = static_cast<const __nv_bfloat16*>(B);
   if (splits > 1) {
     e = cudaMemset2DAsync(C, (size_t)ldc * 4, 0, (size_t)N * 4, M, st);
     if (e != cudaSuccess) return cuda_fail(e, "gemm_bf16: clear C");
-    e = prepare<20, 1>(gemm_bf16_kernel<true>, kGemmSmem);
-    if (e != cudaSuccess) return cuda_fail(e, "gemm_bf16: attributes");
-    gemm_bf16_kernel<true><<<grid, 128, kGemmSmem, st>>>(static_cast<const __nv_bfloat16*>(A), lda,
-                                                         static_cast<const __nv_bfloat16*>(B), ldb, C, ldc, bias, Nt,
-                                                         K / splits, err);
-  } else {
-    e = prepare<20, 0>(gemm_bf16_kernel<false>, kGemmSmem);
-    if (e != cudaSuccess) return cuda_fail(e, "gemm_bf16: attributes");
-    gemm_bf16_kernel<false><<<grid, 128, kGemmSmem, st>>>(static_cast<const __nv_bfloat16*>(A), lda,
-                                                          static_cast<const __nv_bfloat16*>(B), ldb, C, ldc, bias,
-                                                          Nt, K, err);
   }
+#define G1_GEMM_LAUNCH(AT, M_T, KEY)                                                              \
+  do {                                                                                           \
+    if ((e = prepare<20, KEY>(gemm_bf16_kernel<AT, M_T>, gemm_smem<M_T>())) != cudaSuccess)      \
+      return cuda_fail(e, "gemm_bf16: attributes");                                              \
+    gemm_bf16_kernel<AT, M_T><<<grid, 128, gemm_smem<M_T>(), st>>>(a, lda, b, ldb, C, ldc, bias, Nt, \
+                                                                  K / splits, err);              \
+  } while (0)
+  if (splits > 1) {
+    if (MT == 2) G1_GEMM_LAUNCH(true, 2, 3); else G1_GEMM_LAUNCH(true, 1, 1);
+  } else {
+    if (MT == 2) G1_GEMM_LAUNCH(false, 2, 2); else G1_GEMM_LAUNCH(false, 1, 0);
+  }
+#undef G1_GEMM_LAUNCH
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : cuda_fail(e, "gemm_bf16_kernel");
 }
