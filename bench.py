@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
-    p.add_argument("--surrogate-steps", type=int, default=300, help="training steps of the surrogate (-1: skip)")
+    p.add_argument("--surrogate-steps", type=int, default=1000, help="training steps of the surrogate (-1: skip)")
     return p.parse_args()
 
 
@@ -365,7 +365,7 @@ def surrogate_bench(device, train_steps, world):
     for k in range(train_steps):
         idx = torch.randint(0, X.shape[0], (SUR_BATCH,), generator=g, device=device)
         xb = X[idx].contiguous()
-        lr = 1e-3 * (0.1 ** (k / max(train_steps, 1)))
+        lr = 2e-3 * (0.05 ** (k / max(train_steps, 1)))
         hist.append(sur.train_step(xb, xb.T.contiguous(), T[idx].contiguous(), lr=lr))
     torch.cuda.synchronize()
     l1 = float(hist[-1].item()) if hist else l0
