@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--surrogate-steps", type=int, default=1000, help="training steps of the surrogate (-1: skip)")
+    p.add_argument("--part", default="all", choices=["all", "policy", "adjoint", "gemm"],
+                   help="one sub-benchmark alone on --nenv envs (rows), one GPU (a small case for a profiler)")
+    p.add_argument("--horizon", type=int, default=64, help="adjoint horizon with --part adjoint")
     return p.parse_args()
 
 
@@ -261,24 +264,25 @@ def policy_fused_bench(n, rank, device, stream, steps, warmup, world, local, ini
 ADJ_ENVS, ADJ_H, ADJ_C = 4096, 64, 8
 
 
-def adjoint_bench(device, stream, steps, warmup, world):
+def adjoint_bench(device, stream, steps, warmup, world, n=ADJ_ENVS, horizon=ADJ_H):
     """Loss and gradients over a 64-step horizon at dt 2 ms for 4,096 envs
     (targets 64 x 29 and per-env kp / kd scales U[0.8, 1.2]), checkpoints
-    every 8 steps: forward rollout + reverse sweep, one g1b_adjoint call."""
+    every 8 steps: forward rollout + reverse sweep, one g1b_adjoint call.
+    n and horizon change the envs and the horizon (smaller profiler cases)."""
     import torch
     from g1sim_b200 import adjoint as A
     from g1sim_b200.model import g1_model_data as M
     rng = np.random.default_rng(0)
-    n = ADJ_ENVS
+    H = horizon
     stand = np.asarray(M.qpos_stand)
     q0 = np.repeat(stand[:, None], n, axis=1)
     q0[2] = 0.79
     q0[7:] += rng.normal(0, 0.02, size=(29, n))
     f = lambda x: torch.tensor(np.ascontiguousarray(x), dtype=torch.float32, device=device)  # noqa: E731
-    tg = f(stand[7:][None, :, None] + rng.normal(0, 0.05, size=(ADJ_H, 29, n)))
+    tg = f(stand[7:][None, :, None] + rng.normal(0, 0.05, size=(H, 29, n)))
     kp, kd = f(rng.uniform(0.8, 1.2, n)), f(rng.uniform(0.8, 1.2, n))
     qp, qv, an = f(q0), f(np.zeros((35, n))), f(np.full((16, n), 1e30))
-    scratch = torch.empty(A.scratch_size(n, ADJ_H, ADJ_C), dtype=torch.float32, device=device)
+    scratch = torch.empty(A.scratch_size(n, H, ADJ_C), dtype=torch.float32, device=device)
 
     def one():
         with torch.cuda.stream(stream):
@@ -298,9 +302,9 @@ def adjoint_bench(device, stream, steps, warmup, world):
         t, r = one()
         times.append(t)
     ms = max_over_ranks(statistics.mean(times), world, device)
-    return {"value": float(n) * ADJ_H * world / (ms * 1e-3), "unit": "env-steps/s (horizon steps differentiated)",
-            "ms_per_call": ms, "config": {"envs": n, "horizon": ADJ_H, "checkpoint": ADJ_C, "dt": DT,
-                                         "decision_variables": "targets 64x29 + kp/kd scale per env"},
+    return {"value": float(n) * H * world / (ms * 1e-3), "unit": "env-steps/s (horizon steps differentiated)",
+            "ms_per_call": ms, "config": {"envs": n, "horizon": H, "checkpoint": ADJ_C, "dt": DT,
+                                         "decision_variables": f"targets {H}x29 + kp/kd scale per env"},
             "kernels": "adj_forward, adj_segment, adj_vjp (Dual<float,4>, 30 tangent blocks per env), adj_accum",
             "finite": bool(torch.isfinite(r["grad_targets"]).all().item())}
 
@@ -385,6 +389,52 @@ def surrogate_bench(device, train_steps, world):
             "fallback_rollout": {"envs": SUR_ENVS, "steps": 50, "bound": 1e-3,
                                  "fraction_surrogate": frac, "one_step_error": err},
             "gemm_status": S.gemm_status()}
+
+
+def gemm_bench(device, rows, steps, warmup):
+    """One surrogate hidden-layer product alone: C[rows x 512] = A[rows x 512]
+    . W[512 x 512]^T + b (g1b_gemm_bf16), timed over `steps` calls."""
+    import torch
+    from g1sim_b200 import surrogate as S
+    g = torch.Generator(device=device).manual_seed(0)
+    A_ = torch.randn(rows, 512, device=device, generator=g).to(torch.bfloat16)
+    W = torch.randn(512, 512, device=device, generator=g).to(torch.bfloat16)
+    b = torch.randn(512, device=device, generator=g)
+    C_ = torch.empty(rows, 512, device=device)
+    for _ in range(max(1, warmup)):
+        S.gemm(A_, W, C_, bias=b)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(max(1, steps)):
+        S.gemm(A_, W, C_, bias=b)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, steps)
+    return {"shape": [rows, 512, 512], "us_per_call": ms * 1e3,
+            "tflops": 2.0 * rows * 512 * 512 / (ms * 1e-3) / 1e12, "status": S.gemm_status()}
+
+
+def part_only(args, local):
+    """One sub-benchmark alone on one GPU, printed as a diagnostic JSON line
+    (not the bench line): the small cases the profiler captures run this way."""
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device)
+    if args.part == "policy":
+        from g1sim_b200 import workloads
+        w = workloads.randomized(nenv=args.nenv, seed=0)
+        init = {k: torch.tensor(w[k], dtype=torch.float32, device=device)
+                for k in ("qpos", "qvel", "anchor", "ctrl", "mu", "dmass")}
+        r = policy_fused_bench(args.nenv, 0, device, stream, args.steps, args.warmup, 1, local, init)
+    elif args.part == "adjoint":
+        r = adjoint_bench(device, stream, args.steps, args.warmup, 1, n=args.nenv, horizon=args.horizon)
+    else:
+        r = gemm_bench(device, args.nenv, args.steps, args.warmup)
+    print(json.dumps({"part": args.part, "envs_or_rows": args.nenv, **r}))
+    return 0
 
 
 # ------------------------------------------------------------- our arm
@@ -563,6 +613,8 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         return reference_arm(args, world, rank)
+    if args.part != "all":
+        return part_only(args, local)
     return ours(args, world, rank, local)
 
 
