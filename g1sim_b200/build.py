@@ -1,26 +1,32 @@
 """Build libg1cuda.so in-tree with nvcc for sm_100a (B200).
 
-    python -m g1sim_b200.build          # or g1sim_b200.build.build()
+    python -m g1sim_b200.build [--force] [-v]    # or g1sim_b200.build.build()
 
-The library is written next to this file (g1sim_b200/libg1cuda.so) so that
-it travels with the source tree; nothing is installed anywhere else.
+Each translation unit under csrc/ (the plain step, the policy-fused
+rollout, the adjoint, the surrogate) is compiled to an object in parallel,
+then the objects are linked into one shared library written next to this
+file (g1sim_b200/libg1cuda.so), so that it travels with the source tree;
+nothing is installed anywhere else.  A unit is recompiled when it or any
+header it may include is newer than its object.
 """
+import concurrent.futures as cf
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
+OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libg1cuda.so")
-SOURCES = [os.path.join(CSRC, "g1_kernels.cu")]
-DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
+UNITS = ["g1_step.cu", "g1_step_k32.cu", "g1_step_k64.cu", "g1_step_k96.cu", "g1_step_k128.cu", "g1_policy.cu",
+         "g1_adjoint.cu", "g1_surrogate.cu"]
+SOURCES = [os.path.join(CSRC, u) for u in UNITS]
+HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(os.path.dirname(HERE), "include", "g1sim_b200.h")]
+DEPS = SOURCES + HEADERS
 
-NVCC_FLAGS = [
-    "-O3", "-std=c++20", "-lineinfo",
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-Xcompiler", "-fPIC", "-shared",
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++20", "-lineinfo"] + ARCH + ["-Xcompiler", "-fPIC"]
 
 
 def nvcc():
@@ -30,23 +36,45 @@ def nvcc():
     return "nvcc"
 
 
-def stale():
-    if not os.path.exists(LIB):
+def _obj(src):
+    return os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
         return True
-    t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(d) > t for d in DEPS if os.path.exists(d))
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def stale():
+    return _newer(LIB, DEPS)
+
+
+def _compile(src, verbose):
+    obj = _obj(src)
+    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj + ".tmp", src]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n" + r.stdout + r.stderr)
+    os.replace(obj + ".tmp", obj)
+    return r.stdout + r.stderr
 
 
 def build(force=False, verbose=False):
     if not force and not stale():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB + ".tmp"] + SOURCES
+    os.makedirs(OBJDIR, exist_ok=True)
+    todo = [s for s in SOURCES if force or _newer(_obj(s), [s] + HEADERS)]
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        logs = list(ex.map(lambda s: _compile(s, verbose), todo))
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB + ".tmp"] + [_obj(s) for s in SOURCES]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
     if verbose:
-        print(r.stdout + r.stderr)
+        print("\n".join(logs))
     return LIB
 
 
