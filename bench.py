@@ -151,25 +151,46 @@ def barrier(world):
 
 
 # -------------------------------------------------------- CPU baseline
-def cpu_reference(seconds, nenv):
-    """The reference's own FP32 step (oracle/_ref/g1ref_rollout, built from
-    the reference sources) on this host's cores: a bounded sample of the
-    workload, all hardware threads."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "g1ref_rollout")
+def _host_cpus():
+    try:
+        return sorted(os.sched_getaffinity(0))
+    except AttributeError:
+        return list(range(os.cpu_count() or 1))
+
+
+def cpu_reference(seconds, nenv, precision=4):
+    """The reference's own step (oracle/_ref/g1ref_rollout, built from the
+    reference sources; g1ref_rollout64 for its FP64 host build) on this
+    host's CPUs: one single-threaded process per CPU, pinned to it, each on
+    its own contiguous slice of the nenv envs (all 1,000 substeps of each
+    env), until its slice is done or `seconds` have passed.  Throughput =
+    env-steps of all processes / the longest process time."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "g1ref_rollout" if precision == 4 else "g1ref_rollout64")
     if not os.path.exists(exe):
         return None
-    threads = os.cpu_count() or 1
-    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread")
-    out = subprocess.run([exe, "--nenv", str(nenv), "--steps", str(SUBSTEPS), "--decim", str(DECIM),
-                          "--seconds", str(seconds), "--threads", str(threads)],
-                         capture_output=True, text=True, env=env, timeout=seconds * 10 + 120)
-    if out.returncode != 0:
-        return None
-    r = json.loads(out.stdout.strip().splitlines()[-1])
-    return {"value": r["env_steps_per_s"], "unit": "env-steps/s", "cores": r["threads"], "kind": "reference",
-            "sample": (f"first {r['envs']} of the {nenv} envs x {r['substeps']} substeps (dt 2 ms, decimation "
-                       f"10, target redraw, reset at z<0.3; nominal friction/mass: the reference has no "
-                       f"per-env parameters), reference g1_step FP32 via OpenMP, {r['seconds']:.1f} s")}
+    cpus = _host_cpus()
+    per = (nenv + len(cpus) - 1) // len(cpus)
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    procs = []
+    for i, c in enumerate(cpus):
+        cmd = ["taskset", "-c", str(c), exe, "--nenv", str(nenv), "--env0", str(i * per), "--count", str(per),
+               "--steps", str(SUBSTEPS), "--decim", str(DECIM), "--seconds", str(seconds), "--threads", "1"]
+        procs.append(subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=env))
+    res = []
+    for p in procs:
+        out, _ = p.communicate(timeout=seconds * 10 + 120)
+        if p.returncode != 0:
+            return None
+        res.append(json.loads(out.strip().splitlines()[-1]))
+    steps = sum(r["env_steps"] for r in res)
+    wall = max(r["seconds"] for r in res)
+    envs = sum(r["envs"] for r in res)
+    name = "FP32 g1_step" if precision == 4 else "FP64 host build of g1_step"
+    return {"value": steps / wall, "unit": "env-steps/s", "cores": len(cpus), "kind": "reference",
+            "sample": (f"{envs} of the {nenv} envs x {SUBSTEPS} substeps (dt 2 ms, decimation 10, target redraw, "
+                       f"reset at z<0.3; nominal friction/mass: the reference has no per-env parameters), "
+                       f"reference {name}, one pinned single-threaded process per host CPU "
+                       f"({len(cpus)}) on its own env slice, {wall:.1f} s")}
 
 
 def reference_arm(args, world, rank):
@@ -198,6 +219,96 @@ def reference_arm(args, world, rank):
             "e2e": {"value": v, "unit": "env-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+# ------------------------------------------------------- accuracy leg
+ACC_ENVS = 1024
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    import parity
+    return Oracle(), parity
+
+
+def accuracy_plain(state, mu, dmass, device):
+    """Checker, outside the timed region: 1,024 envs sampled evenly from the
+    timed state (after its 1,000 substeps), stepped by the same kernels one
+    substep at a time for one policy step (10 substeps, targets held) and
+    compared with the FP64 oracle from the same float32 state each substep;
+    then the 400-substep drift of a GPU rollout from the oracle's, both from
+    that state."""
+    import torch
+    from g1sim_b200 import _lib
+    from g1sim_b200 import g1sim as G
+    o, parity = _oracle()
+    n = state["qpos"].shape[1]
+    idx = torch.arange(0, n, max(1, n // ACC_ENVS), device=device)[:ACC_ENVS]
+    sub = {k: state[k][:, idx].contiguous() for k in ("qpos", "qvel", "anchor", "ctrl")}
+    smu, sdm = mu[idx].contiguous(), dmass[idx].contiguous()
+    gcfg = _lib.default_config(dt=DT)
+    ocfg = o.config(dt=DT)
+    h = lambda t: t.double().cpu().numpy()  # noqa: E731
+    ctrl, mu64, dm64 = h(sub["ctrl"]), h(smu), h(sdm)
+
+    def read():
+        torch.cuda.synchronize()
+        return h(sub["qpos"]), h(sub["qvel"]), h(sub["anchor"])
+
+    def run(k):
+        G.step(sub["qpos"], sub["qvel"], sub["anchor"], sub["ctrl"], k, config=gcfg, mu=smu, dmass=sdm)
+
+    per = parity.per_substep(o, lambda: run(1), read, ocfg, ctrl, mu=mu64, dmass=dm64, substeps=DECIM)
+    dr = parity.drift(o, run, read, ocfg, ctrl, mu=mu64, dmass=dm64, marks=(10, 100, 400))
+    mapping, block, _ = _lib.get_launch()
+    return {"envs": int(idx.numel()), "per_substep": per, "drift": dr,
+            "kernel": f"g1b_step, launch shape mapping {mapping} block {block} (the timed kernel's physics)",
+            "sample": f"every {max(1, n // ACC_ENVS)}th env of the timed state after {SUBSTEPS} substeps",
+            "metric": "|x - x_fp64| / max(|x_fp64|, 1) per component, from the same float32 state; "
+                      "env-substeps within FP32 rounding of a model switch (oracle margin < 1) excluded"}
+
+
+def accuracy_policy(sim, packed, task, mu, dmass, device):
+    """Checker, outside the timed region: one more policy step of the fused
+    kernel over all envs with action sampling only (no pushes, resets or
+    command redraws, so its 10 substeps run from the pre-step state with the
+    targets the network chose); 1,024 sampled envs are compared with the
+    FP64 oracle's 10 substeps from the same float32 state and targets, and
+    the plain kernel's 10 substeps from that state the same way."""
+    import torch
+    from g1sim_b200 import _lib
+    from g1sim_b200 import g1sim as G
+    from g1sim_b200 import policy as P
+    o, parity = _oracle()
+    n = sim["qpos"].shape[1]
+    idx = torch.arange(0, n, max(1, n // ACC_ENVS), device=device)[:ACC_ENVS]
+    h = lambda t: t.double().cpu().numpy()  # noqa: E731
+    pre = {k: sim[k][:, idx].contiguous() for k in ("qpos", "qvel", "anchor")}
+    pre64 = {k: h(v) for k, v in pre.items()}
+    pr = _lib.policy_default_params()
+    pr.flags = _lib.SAMPLE
+    buf = P.RolloutBuffers(1, n, device)
+    P.policy_rollout(sim, packed, task, buf, 1, decim=DECIM, params=pr, mu=mu, dmass=dmass)
+    torch.cuda.synchronize()
+    ctrl = sim["ctrl"][:, idx].contiguous()
+    fq, fv = h(sim["qpos"][:, idx]), h(sim["qvel"][:, idx])
+    G.step(pre["qpos"], pre["qvel"], pre["anchor"], ctrl, DECIM, config=_lib.default_config(dt=DT),
+           mu=mu[idx].contiguous(), dmass=dmass[idx].contiguous())
+    torch.cuda.synchronize()
+    pq, pv = h(pre["qpos"]), h(pre["qvel"])
+    eq, ev, mg = parity.composed(o, pre64["qpos"], pre64["qvel"], pre64["anchor"], h(ctrl), fq, fv,
+                                 o.config(dt=DT), DECIM, mu=h(mu[idx]), dmass=h(dmass[idx]))
+    # the plain kernel against the oracle from the same start with the same targets
+    eq2, ev2, _ = parity.composed(o, pre64["qpos"], pre64["qvel"], pre64["anchor"], h(ctrl), pq, pv,
+                                  o.config(dt=DT), DECIM, mu=h(mu[idx]), dmass=h(dmass[idx]))
+    st = lambda a: {"median": float(np.median(a)), "p99": float(np.percentile(a, 99)),  # noqa: E731
+                    "max": float(a.max())}
+    return {"envs": int(idx.numel()), "substeps": DECIM,
+            "fused": {"qpos": st(eq), "qvel": st(ev)}, "plain_same_start": {"qpos": st(eq2), "qvel": st(ev2)},
+            "fused_vs_plain_max_abs": float(max(np.abs(fq - pq).max(), np.abs(fv - pv).max())),
+            "metric": "|x - x_fp64| / max(|x_fp64|, 1) after 10 compounded substeps (one policy step), "
+                      "per env the max over components; both from the same float32 state and targets"}
 
 
 # ------------------------------------------------- policy-fused rollout
@@ -250,6 +361,7 @@ def policy_fused_bench(n, rank, device, stream, steps, warmup, world, local, ini
     ms = max_over_ranks(statistics.mean(times), world, device)
     from g1sim_b200 import _lib
     status = _lib.policy_status()
+    acc = accuracy_policy(sim, packed, task, init["mu"], init["dmass"], device) if rank == 0 else None
     env_steps = float(n) * SUBSTEPS
     net_flops = 2.0 * (ACTOR_MACS + CRITIC_MACS) * n * (SUBSTEPS // DECIM)
     return {"value": env_steps * world / (ms * 1e-3), "unit": "env-steps/s", "ms_per_step": ms,
@@ -257,7 +369,7 @@ def policy_fused_bench(n, rank, device, stream, steps, warmup, world, local, ini
             "network_tflops": net_flops / (ms * 1e-3) / 1e12,
             "network_flops_per_env_policy_step": 2.0 * (ACTOR_MACS + CRITIC_MACS),
             "outputs": "obs, actions, log-probs, values, rewards, dones, resets, bootstrap value",
-            "status": status, "finite": bool(torch.isfinite(buf.rewards).all().item())}
+            "status": status, "finite": bool(torch.isfinite(buf.rewards).all().item()), "accuracy": acc}
 
 
 # ------------------------------------------------------- horizon adjoint
@@ -500,10 +612,13 @@ def ours(args, world, rank, local):
     timed_steps(args.warmup)
     barrier(world)
     torch.cuda.synchronize()
+    rc0 = int(rc.sum().item())
     with ClockSampler(local) as clk:
         times = timed_steps(args.steps)
     torch.cuda.synchronize()
     barrier(world)
+    resets_per_step = (int(rc.sum().item()) - rc0) / max(args.steps, 1)
+    accuracy = accuracy_plain(st, init["mu"], init["dmass"], device) if rank == 0 else None
     ms = max_over_ranks(statistics.mean(times), world, device)
     env_steps = float(n) * SUBSTEPS
     value = env_steps * world / (ms * 1e-3)
@@ -559,7 +674,6 @@ def ours(args, world, rank, local):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world, device)
     e2e_value = env_steps * world / e2e_s
 
-    resets = int(rc.sum().item())
     finite = bool(torch.isfinite(st["qpos"]).all().item())
 
     pol = policy_fused_bench(n, rank, device, stream, args.steps, args.warmup, world, local, init)
@@ -569,6 +683,10 @@ def ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference(args.cpu_seconds, n)
+        fp64 = cpu_reference(args.cpu_seconds / 2, n, precision=8)
+        if cpu is not None and fp64 is not None:
+            cpu["fp64_host"] = {"value": fp64["value"], "unit": fp64["unit"], "cores": fp64["cores"],
+                                "sample": fp64["sample"]}
 
     if rank == 0:
         line = {
@@ -591,7 +709,7 @@ def ours(args, world, rank, local):
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
             "single_launch": {"value": env_steps / (single_ms * 1e-3), "ms": single_ms},
-            "resets_last_step": resets, "finite": finite,
+            "resets_per_timed_step": resets_per_step, "finite": finite, "accuracy": accuracy,
             "policy_fused": pol,
         }
         if adj is not None:

@@ -6,11 +6,12 @@ Each translation unit under csrc/ (the plain step, the policy-fused
 rollout, the adjoint, the surrogate) is compiled to an object in parallel,
 then the objects are linked into one shared library written next to this
 file (g1sim_b200/libg1cuda.so), so that it travels with the source tree;
-nothing is installed anywhere else.  A unit is recompiled when it or any
-header it may include is newer than its object.
+nothing is installed anywhere else.  A unit is recompiled when it or a
+header it includes (transitively) is newer than its object.
 """
 import concurrent.futures as cf
 import os
+import re
 import subprocess
 import sys
 
@@ -51,6 +52,21 @@ def stale():
     return _newer(LIB, DEPS)
 
 
+def _includes(path, seen=None):
+    """Files under csrc/ and include/ that `path` includes, transitively."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', text, re.M):
+        dep = os.path.normpath(os.path.join(os.path.dirname(path), name))
+        if dep not in seen and os.path.exists(dep):
+            seen.add(dep)
+            _includes(dep, seen)
+    return seen
+
+
 def _compile(src, verbose):
     obj = _obj(src)
     cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj + ".tmp", src]
@@ -65,7 +81,7 @@ def build(force=False, verbose=False):
     if not force and not stale():
         return LIB
     os.makedirs(OBJDIR, exist_ok=True)
-    todo = [s for s in SOURCES if force or _newer(_obj(s), [s] + HEADERS)]
+    todo = [s for s in SOURCES if force or _newer(_obj(s), [s] + sorted(_includes(s)))]
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
         logs = list(ex.map(lambda s: _compile(s, verbose), todo))
     cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB + ".tmp"] + [_obj(s) for s in SOURCES]

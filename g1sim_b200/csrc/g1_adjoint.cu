@@ -94,24 +94,15 @@ constexpr size_t kNoAllocScratchFloats = size_t(1) << 21;  // 8 MiB of float
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
 
 namespace {
-// Device address of the array, looked up once per device (the host-side
-// name of a __device__ array is not a device address).
-std::mutex g_noalloc_mu;
-float* g_noalloc_ptr[64] = {};
-
+// Device address of the array on the current device.  The host-side name of
+// a __device__ array is not a device address; the address is looked up on
+// every call (a cheap query once the module is loaded), so it stays right
+// after a cudaDeviceReset re-creates the context.
 int noalloc_scratch(float** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_fail(e, "adjoint_noalloc: cudaGetDevice");
-  if (dev < 0 || dev >= 64) return fail("adjoint_noalloc: device index out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "adjoint_noalloc: cudaGetSymbolAddress");
-    g_noalloc_ptr[dev] = static_cast<float*>(p);
-  }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "adjoint_noalloc: cudaGetSymbolAddress");
+  *out = static_cast<float*>(p);
   return 0;
 }
 }  // namespace

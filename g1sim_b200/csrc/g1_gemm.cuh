@@ -142,8 +142,10 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
       float v[32];
       tc::tmem_ld32(lane_base + (uint32_t)c, v);
       if (bias && blockIdx.z == 0) {
+        const int nb = Nt - c < 32 ? Nt - c : 32;  // the bias holds exactly N floats
 #pragma unroll
-        for (int i = 0; i < 32; ++i) v[i] += __ldg(bias + n0 + c + i);
+        for (int i = 0; i < 32; ++i)
+          if (i < nb) v[i] += __ldg(bias + n0 + c + i);
       }
       if (c + 32 > Nt) {  // Nt = 16 or 48 ...: partial last group
         for (int i = 0; i < Nt - c; ++i) {

@@ -13,9 +13,12 @@
 // compile-time constants, src/g1_model.h:80,351), so this harness runs every
 // env with the nominal model; the work per substep is the same.
 //
-// Envs are processed in chunks across the threads until --seconds of wall
-// time have passed (a bounded sample of the workload); it prints one JSON
-// line with env-steps/s.
+// Envs env0 .. env0 + count - 1 are processed in chunks across the threads
+// until they are done or --seconds of wall time have passed (a bounded
+// sample of the workload); it prints one JSON line with env-steps/s.  The
+// CPU baseline runs one such process per host core, pinned to that core,
+// each on its own slice of the envs.  Built at G1_PRECISION=4 (the
+// reference's FP32 step) and at G1_PRECISION=8 (its FP64 host build).
 #include "g1_core.h"
 
 #include <omp.h>
@@ -37,7 +40,7 @@ static float uniform24(unsigned seed, unsigned stream, unsigned counter) {
 }
 
 int main(int argc, char** argv) {
-  int nenv = 65536, nsteps = 1000, decim = 10, threads = 0;
+  int nenv = 65536, nsteps = 1000, decim = 10, threads = 0, env0 = 0, count = -1;
   double seconds = 10.0, dt = 2e-3;
   unsigned seed = 0;
   for (int i = 1; i < argc; ++i) {
@@ -47,7 +50,11 @@ int main(int argc, char** argv) {
     else if (!strcmp(argv[i], "--threads")) threads = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--seconds")) seconds = atof(argv[++i]);
     else if (!strcmp(argv[i], "--seed")) seed = (unsigned)atoi(argv[++i]);
+    else if (!strcmp(argv[i], "--env0")) env0 = atoi(argv[++i]);
+    else if (!strcmp(argv[i], "--count")) count = atoi(argv[++i]);
   }
+  if (count < 0) count = nenv - env0;
+  const int env_end = env0 + count < nenv ? env0 + count : nenv;
   if (threads > 0) omp_set_num_threads(threads);
   int nthr = omp_get_max_threads();
   const int npolicy = nsteps / decim;
@@ -59,8 +66,8 @@ int main(int argc, char** argv) {
   double t0 = omp_get_wtime(), elapsed = 0;
   int chunk = nthr * 4;
   double zsum = 0;
-  for (int base = 0; base < nenv; base += chunk) {
-    int hi = base + chunk < nenv ? base + chunk : nenv;
+  for (int base = env0; base < env_end; base += chunk) {
+    int hi = base + chunk < env_end ? base + chunk : env_end;
     long long rs = 0;
     double zs = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : rs, zs)
@@ -96,9 +103,10 @@ int main(int argc, char** argv) {
     if (elapsed >= seconds) break;
   }
   double env_steps = (double)envs_done * npolicy * decim;
-  printf("{\"env_steps_per_s\": %.6g, \"threads\": %d, \"envs\": %lld, \"substeps\": %d, "
-         "\"seconds\": %.4f, \"resets\": %lld, \"mean_z\": %.5f, \"dt\": %g, \"decim\": %d}\n",
-         env_steps / elapsed, nthr, envs_done, npolicy * decim, elapsed, resets,
-         zsum / (double)(envs_done > 0 ? envs_done : 1), dt, decim);
+  printf("{\"env_steps_per_s\": %.6g, \"env_steps\": %.6g, \"threads\": %d, \"envs\": %lld, "
+         "\"env0\": %d, \"substeps\": %d, \"seconds\": %.4f, \"resets\": %lld, \"mean_z\": %.5f, "
+         "\"dt\": %g, \"decim\": %d, \"precision\": %d}\n",
+         env_steps / elapsed, env_steps, nthr, envs_done, env0, npolicy * decim, elapsed, resets,
+         zsum / (double)(envs_done > 0 ? envs_done : 1), dt, decim, (int)sizeof(G1Real));
   return 0;
 }

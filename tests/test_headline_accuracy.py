@@ -1,0 +1,92 @@
+"""Accuracy of the plain step at the benchmark's full size (needs a B200).
+
+The randomised workload at 65,536 envs (dt 2 ms, decimation 10, per-env
+friction and base mass, targets redrawn every policy step, in-kernel resets)
+is advanced 20 policy steps so that the envs are spread over standing,
+stepping, slipping and falling states; then every one of the 65,536 envs is
+checked against the FP64 oracle:
+
+  * one substep at a time for a policy step (10 substeps, targets held),
+    both sides from the GPU's float32 state each substep: qpos within 1e-6,
+    qvel within 1e-5 (median 1e-6) -- the metric's 1e-5 bound per step;
+  * one decimated policy step (target redraw, 10 compounded substeps, reset
+    check) against the oracle's rollout from the same state: the compounded
+    error stays at the per-step level times the substeps.
+"""
+import numpy as np
+import pytest
+import torch
+
+from g1sim_b200 import workloads
+from g1sim_b200 import g1sim as G
+from g1sim_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+N = 65536
+
+
+def host(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+@pytest.fixture(scope="module")
+def mid_rollout():
+    w = workloads.randomized(nenv=N, seed=0)
+    st = {k: torch.tensor(w[k], dtype=torch.float32, device=DEV) for k in ("qpos", "qvel", "anchor", "ctrl")}
+    mu = torch.tensor(w["mu"], dtype=torch.float32, device=DEV)
+    dm = torch.tensor(w["dmass"], dtype=torch.float32, device=DEV)
+    rc = torch.zeros(N, dtype=torch.int32, device=DEV)
+    G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 20, 10, seed=0, step0=0, mu=mu, dmass=dm,
+              reset_count=rc)
+    torch.cuda.synchronize()
+    assert int(rc.sum()) > 0  # the spread includes falls and resets
+    return st, mu, dm, w
+
+
+def test_per_substep_parity_all_envs(oracle, mid_rollout):
+    import parity
+    st, mu, dm, w = mid_rollout
+    s = {k: v.clone() for k, v in st.items()}
+    cfg = _lib.default_config(dt=2e-3)
+
+    def read():
+        torch.cuda.synchronize()
+        return host(s["qpos"]), host(s["qvel"]), host(s["anchor"])
+
+    r = parity.per_substep(oracle, lambda: G.step(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], 1, config=cfg,
+                                                  mu=mu, dmass=dm),
+                           read, oracle.config(dt=2e-3), host(s["ctrl"]), mu=w["mu"].astype(np.float64),
+                           dmass=w["dmass"].astype(np.float64), substeps=10)
+    print(r)
+    assert r["env_substeps"] == 10 * N
+    assert r["near_branch_fraction"] < 0.01
+    assert r["qpos_max"] < 1e-6
+    assert r["qvel_max"] < 1e-5
+    assert r["qvel_median"] < 1e-6
+    assert r["anchor_max_m"] < 1e-6
+
+
+def test_policy_step_parity_all_envs(oracle, mid_rollout):
+    from oracle import RolloutParams
+    st, mu, dm, w = mid_rollout
+    s = {k: v.clone() for k, v in st.items()}
+    q64, v64, a64, c64 = (host(s[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
+    rc64 = np.zeros(N, dtype=np.int32)
+    margin = oracle.branch_margin(oracle.config(dt=2e-3), q64, v64, a64, c64, mu=w["mu"].astype(np.float64),
+                                  dmass=w["dmass"].astype(np.float64))
+    oracle.rollout_soa(1, 10, oracle.config(dt=2e-3), RolloutParams(0, 20, 0.3, 0.3, 0.75, 0.85, 1), q64, v64, a64,
+                       c64, mu=w["mu"].astype(np.float64), dmass=w["dmass"].astype(np.float64), reset_count=rc64)
+    rc = torch.zeros(N, dtype=torch.int32, device=DEV)
+    G.rollout(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], 1, 10, seed=0, step0=20, mu=mu, dmass=dm, reset_count=rc)
+    torch.cuda.synchronize()
+    assert np.array_equal(s["ctrl"].cpu().numpy().astype(np.float64), c64)  # redrawn targets bit-exact
+    keep = (rc64 == 0) & (rc.cpu().numpy() == 0) & (margin >= 1.0)
+    eq = (np.abs(host(s["qpos"]) - q64) / np.maximum(np.abs(q64), 1)).max(axis=0)[keep]
+    ev = (np.abs(host(s["qvel"]) - v64) / np.maximum(np.abs(v64), 1)).max(axis=0)[keep]
+    print(f"policy step, {keep.sum()} envs: qpos max {eq.max():.2e} median {np.median(eq):.2e}; qvel max "
+          f"{ev.max():.2e} p99 {np.percentile(ev, 99):.2e} median {np.median(ev):.2e}")
+    assert keep.mean() > 0.95
+    assert np.median(ev) < 1e-5
+    assert np.percentile(ev, 99) < 1e-4

@@ -39,12 +39,16 @@ def bf(x):
 
 
 @pytest.mark.parametrize("M_,N,K,splits", [(256, 512, 512, 1), (128, 64, 512, 1), (384, 128, 128, 1),
-                                           (128, 512, 8192, 16), (512, 128, 4096, 8)])
+                                           (128, 512, 8192, 16), (512, 128, 4096, 8), (128, 16, 128, 1),
+                                           (256, 48, 256, 1), (256, 48, 512, 2)])
 def test_gemm_matches_fp64(M_, N, K, splits):
     g = torch.Generator(device=DEV).manual_seed(M_ + N + K)
     A = bf(torch.randn(M_, K, device=DEV, generator=g))
     B = bf(torch.randn(N, K, device=DEV, generator=g))
-    bias = torch.randn(N, device=DEV, generator=g)
+    # the bias holds exactly N floats, followed by NaN: a read past its end shows in C
+    fence = torch.full((N + 64,), float("nan"), device=DEV)
+    fence[:N] = torch.randn(N, device=DEV, generator=g)
+    bias = fence[:N]
     C_ = torch.full((M_, N), 7.0, device=DEV)
     S.gemm(A, B, C_, bias=bias, splits=splits)
     torch.cuda.synchronize()
