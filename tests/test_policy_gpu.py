@@ -162,8 +162,8 @@ def test_policy_step_physics_matches_oracle(net, oracle):
     oracle.step_soa(10, oracle.config(dt=2e-3), q64, v64, a64, host(sim["ctrl"]), outputs=False)
     eq, ev = relerr(host(sim["qpos"]), q64), relerr(host(sim["qvel"]), v64)
     print(f"policy-step physics qpos max {eq.max():.2e} qvel max {ev.max():.2e}")
-    assert eq.max() < 1e-6
-    assert ev.max() < 1e-4
+    assert eq.max() < 1e-6  # measured 1.7e-7
+    assert ev.max() < 5e-5  # 10 compounded substeps after a push (measured 5.9e-6)
     t = task.push_timer.cpu().numpy()
     assert ((t >= 50) & (t < 150)).all()
 
