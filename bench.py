@@ -417,7 +417,8 @@ def adjoint_bench(device, stream, steps, warmup, world, n=ADJ_ENVS, horizon=ADJ_
     return {"value": float(n) * H * world / (ms * 1e-3), "unit": "env-steps/s (horizon steps differentiated)",
             "ms_per_call": ms, "config": {"envs": n, "horizon": H, "checkpoint": ADJ_C, "dt": DT,
                                          "decision_variables": f"targets {H}x29 + kp/kd scale per env"},
-            "kernels": "adj_forward, adj_segment, adj_vjp (Dual<float,4>, 30 tangent blocks per env), adj_accum",
+            "kernels": "adj_kernel<float, 32> (one launch: forward rollout with checkpoints, then per segment the "
+                       "recomputed states and the reverse-mode product of each step; tape in shared memory)",
             "finite": bool(torch.isfinite(r["grad_targets"]).all().item())}
 
 

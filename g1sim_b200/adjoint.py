@@ -6,10 +6,13 @@
 The loss of env e over H single-substep steps (dt from the config) is
     L_e = sum_{t=1..H} (z_t - z_ref)^2 + w_track * |q_t - u_{t-1}|^2
 with z the base height and q the 29 joint angles; u_t the PD targets of
-step t.  Forward and backward run in one call of g1b_adjoint (the CUDA
-reverse sweep with checkpoints every `checkpoint` steps); the autograd
-Function keeps its gradients for backward.  Arrays are SoA with the env
-axis last, as in G1Sim: targets (H, 29, nenv), qpos0 (36, nenv), ...
+step t.  Forward and backward run in one call of g1b_adjoint (one CUDA
+launch: the forward rollout with checkpoints every `checkpoint` steps, then
+the hand-derived reverse-mode sweep of the step, segment by segment); the
+autograd Function keeps its gradients for backward.  kp_scale / kd_scale
+may be None (scales of 1; no gradient is returned for them).  Arrays are SoA
+with the env axis last, as in G1Sim: targets (H, 29, nenv), qpos0 (36,
+nenv), ...
 """
 import ctypes as C
 
@@ -65,17 +68,18 @@ class HorizonLoss(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, targets, kp_scale, kd_scale, qpos0, qvel0, anchor0, checkpoint, z_ref, w_track, config):
-        r = horizon_adjoint(targets.detach().contiguous(), kp_scale.detach().contiguous(),
-                            kd_scale.detach().contiguous(), qpos0.detach().contiguous(),
-                            qvel0.detach().contiguous(), anchor0.detach().contiguous(), checkpoint, z_ref,
+        d = lambda t: None if t is None else t.detach().contiguous()  # noqa: E731
+        r = horizon_adjoint(d(targets), d(kp_scale), d(kd_scale), d(qpos0), d(qvel0), d(anchor0), checkpoint, z_ref,
                             w_track, config)
+        ctx.has_kp, ctx.has_kd = kp_scale is not None, kd_scale is not None
         ctx.save_for_backward(r["grad_targets"], r["grad_kp"], r["grad_kd"], r["grad_qpos0"], r["grad_qvel0"])
         return r["loss"]
 
     @staticmethod
     def backward(ctx, g):
         gt, gkp, gkd, gq, gv = ctx.saved_tensors
-        return gt * g, gkp * g, gkd * g, gq * g, gv * g, None, None, None, None, None
+        return (gt * g, gkp * g if ctx.has_kp else None, gkd * g if ctx.has_kd else None, gq * g, gv * g, None, None,
+                None, None, None)
 
 
 def horizon_loss(targets, kp_scale, kd_scale, qpos0, qvel0, anchor0, checkpoint=8, z_ref=0.78, w_track=0.1,

@@ -192,10 +192,11 @@ int g1b_policy_status(int* code);
  * over H single-substep steps x_{t+1} = step(x_t, u_t, kp_scale, kd_scale)
  * (x = qpos, qvel, anchor; friction 1, no base-mass offset), with respect
  * to the PD targets u_t, the per-env gain scales and the initial state.
- * Reverse sweep with checkpoints every `checkpoint` steps and recomputation
- * in between; each step's vector-Jacobian product is exact to rounding (the
- * derivative of the step as computed, one-sided at contact / clamp
- * switches). */
+ * One launch per call: the forward rollout keeps a checkpoint every
+ * `checkpoint` steps, then each segment is recomputed from its checkpoint
+ * and reversed step by step with a hand-derived reverse-mode product of the
+ * step (exact to rounding: the derivative of the step as computed,
+ * one-sided at contact / clamp switches). */
 typedef struct g1b_adjoint_problem {
   int horizon;     /* H */
   int checkpoint;  /* keep the state every `checkpoint` steps */
@@ -203,7 +204,7 @@ typedef struct g1b_adjoint_problem {
   float w_track;   /* weight of the joint tracking term (0.1) */
 } g1b_adjoint_problem;
 /* Scratch elements (float, or double for the _f64 variant) that g1b_adjoint
- * needs for nenv envs: ((ceil(H/C) + 1) * 87 + C * 87 + 87 + 120) * nenv. */
+ * needs for nenv envs: (ceil(H/C) + 1 + C) * 87 * nenv. */
 int g1b_adjoint_scratch_size(int nenv, const g1b_adjoint_problem* pr, size_t* count);
 /* Arrays SoA with the env axis fastest: qpos0 [36][nenv], qvel0 [35][nenv],
  * anchor0 [16][nenv], targets / grad_targets [H][29][nenv], kp_scale,
@@ -225,7 +226,7 @@ int g1b_adjoint_f64(int nenv, const g1b_config* cfg, const g1b_adjoint_problem* 
  * start-up, or a host whose device memory is owned by another allocator
  * and that cannot pass a buffer): the same FP32 computation, with the
  * workspace in one fixed device array of g1b_adjoint_noalloc_capacity()
- * floats (8 MiB; at horizon 64 and checkpoint 8 that is up to 1,243 envs)
+ * floats (8 MiB; at horizon 64 and checkpoint 8 that is up to 1,418 envs)
  * instead of caller scratch.  Larger problems are rejected with a message
  * in g1b_last_error().  The library allocates nothing: every device that
  * loads it holds the array until the process exits.  The first call on a

@@ -2,14 +2,19 @@
 
 Reference values come from the FP64 oracle on the CPU: the loss of a
 64-step rollout, and central finite differences of it (h = 1e-6) with
-respect to PD targets, gain scales and the initial state.
+respect to PD targets, gain scales and the initial state, on all 16 envs of
+the workload's FD sample and on problems whose trajectories cross the
+model's switches: feet touching down during the horizon, feet slipping
+under a base push, joints driven past their soft limits.
 
   * FP64 device build (g1b_adjoint_f64): loss to 1e-6 relative (the device
     contracts a*b+c into FMAs, the oracle does not; 64 steps of stiff
     contact dynamics grow that 1e-16 difference to ~2e-7), gradients
     to 1e-4 relative of the FD value (FD truncation and rounding at h = 1e-6
-    are ~1e-7 here; the margin covers steps that pass near a contact or
-    clamp switch, where both sides use one-sided derivatives);
+    are ~1e-7 here).  Where an FD stencil straddles a switch (its one-sided
+    differences disagree) it is repeated with h = 1e-7: the adjoint is the
+    derivative along the branch taken (measured: 1 of 56 stencils on the
+    touchdown problem, which then agrees to 1e-8);
   * FP32 kernels (g1b_adjoint): loss to 1e-4, gradient fields to 1e-3 in
     relative 2-norm and cosine > 0.9999 against the FP64 build (measured
     ~4e-6 on this settled standing problem);
@@ -28,14 +33,17 @@ from g1sim_b200.model import g1_model_data as M
 pytestmark = pytest.mark.gpu
 
 DEV = torch.device("cuda", 0)
-H, NENV = 64, 16
+H, NENV = 64, 16  # the workload's horizon and its FD sample of 16 envs
 STAND = np.asarray(M.qpos_stand)
 
 
-def problem(golden_host, n=NENV, seed=0):
+def problem(golden_host, n=NENV, seed=0, kind="stand"):
     """Settled standing states (the reference's own settling run) with small
     joint / velocity perturbations; targets = stand + N(0, 0.05) per step;
-    gain scales U[0.8, 1.2]."""
+    gain scales U[0.8, 1.2].  kind "touchdown": the stand pose 2-3 cm above
+    the ground with free anchors (the feet land during the horizon); "slip":
+    the standing state pushed sideways at 0.5-0.7 m/s (the feet slide);
+    "limits": targets past the joint ranges on both sides (soft limits)."""
     rng = np.random.default_rng(seed)
     q0 = np.repeat(golden_host["settle_qpos"][:, None], n, axis=1)
     v0 = np.repeat(golden_host["settle_qvel"][:, None], n, axis=1)
@@ -43,6 +51,22 @@ def problem(golden_host, n=NENV, seed=0):
     q0[7:] += rng.normal(0, 0.01, size=(29, n))
     v0[6:] += rng.normal(0, 0.05, size=(29, n))
     tg = STAND[7:, None, None].transpose(1, 0, 2) + rng.normal(0, 0.05, size=(H, 29, n))
+    if kind == "touchdown":
+        q0[:] = STAND[:, None]
+        q0[2] = STAND[2] + rng.uniform(0.0, 0.01, n)
+        q0[7:] += rng.normal(0, 0.01, size=(29, n))
+        v0[:] = 0.0
+        a0[:] = 1e30
+    elif kind == "slip":
+        ang = rng.uniform(0, 2 * np.pi, n)
+        sp = rng.uniform(0.5, 0.7, n)
+        v0[0] += sp * np.cos(ang)
+        v0[1] += sp * np.sin(ang)
+    elif kind == "limits":
+        rngs = np.asarray(M.jnt_range)
+        for j in (3, 9, 16, 23):  # knees and shoulders: past the lower, then the upper limit
+            tg[: H // 2, j] = rngs[j, 0] - 0.3
+            tg[H // 2:, j] = rngs[j, 1] + 0.3
     kp = rng.uniform(0.8, 1.2, n)
     kd = rng.uniform(0.8, 1.2, n)
     f32 = lambda x: np.asarray(x, np.float32).astype(np.float64)  # noqa: E731  (exact in both precisions)
@@ -91,39 +115,113 @@ def test_loss_matches_oracle(prob, r64, oracle):
         assert abs(r64["loss"][e] - ref) <= 1e-6 * abs(ref), (e, r64["loss"][e], ref)
 
 
-def test_fp64_gradients_match_central_differences(prob, r64, oracle):
-    rng = np.random.default_rng(5)
-    h = 1e-6
+def central(f, h=1e-6):
+    """Central difference of f(step) at 0 with step h (the workload's FD
+    step).  Where the stencil straddles a switch of the model (the central
+    differences at h and h / 2 disagree by more than their truncation and
+    rounding errors), the difference is taken again with h / 10: the adjoint
+    is the derivative along the branch taken, which a stencil across the
+    switch does not measure."""
+    f0 = f(0.0)
+    c1 = (f(h) - f(-h)) / (2 * h)
+    c2 = (f(h / 2) - f(-h / 2)) / h
+    noise = 8 * np.finfo(np.float64).eps * abs(f0) / h
+    if abs(c1 - c2) <= 1e-6 * max(abs(c1), 1e-3) + noise:
+        return c1, False
+    return (f(h / 10) - f(-h / 10)) / (2 * h / 10), True
+
+
+def fd_errors(prob, r64, oracle, envs, seed=5, ntargets=3, straddled=None):
+    rng = np.random.default_rng(seed)
     errs = []
-    for e in range(4):
+    note = (lambda s: straddled.append(s)) if straddled is not None else (lambda s: None)  # noqa: E731
+
+    def check(ad, f):
+        fd, st = central(f)
+        note(st)
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-3))
+
+    for e in envs:
         # individual targets
-        for _ in range(6):
+        for _ in range(ntargets):
             t, j = int(rng.integers(H)), int(rng.integers(29))
-            tp, tm = prob["tg"].copy(), prob["tg"].copy()
-            tp[t, j, e] += h
-            tm[t, j, e] -= h
-            fd = (oracle_loss(oracle, prob, e, tg=tp) - oracle_loss(oracle, prob, e, tg=tm)) / (2 * h)
-            errs.append(abs(r64["grad_targets"][t, j, e] - fd) / max(abs(fd), 1e-3))
+
+            def ft(x, t=t, j=j):
+                tg = prob["tg"].copy()
+                tg[t, j, e] += x
+                return oracle_loss(oracle, prob, e, tg=tg)
+            check(r64["grad_targets"][t, j, e], ft)
         # gain scales
         for key, gk in (("kp", "grad_kp"), ("kd", "grad_kd")):
-            x = prob[key][e]
-            fd = (oracle_loss(oracle, prob, e, **{key: x + h}) - oracle_loss(oracle, prob, e, **{key: x - h})) / (2 * h)
-            errs.append(abs(r64[gk][e] - fd) / max(abs(fd), 1e-3))
+            x0 = prob[key][e]
+            check(r64[gk][e], lambda x, key=key, x0=x0: oracle_loss(oracle, prob, e, **{key: x0 + x}))
         # a random direction over all targets
         d = rng.normal(size=prob["tg"].shape) * (np.arange(prob["tg"].shape[2]) == e)
-        fd = (oracle_loss(oracle, prob, e, tg=prob["tg"] + h * d) - oracle_loss(oracle, prob, e, tg=prob["tg"] - h * d)) / (2 * h)
-        ad = float(np.sum(r64["grad_targets"][:, :, e] * d[:, :, e]))
-        errs.append(abs(ad - fd) / max(abs(fd), 1e-3))
+        check(float(np.sum(r64["grad_targets"][:, :, e] * d[:, :, e])),
+              lambda x, d=d: oracle_loss(oracle, prob, e, tg=prob["tg"] + x * d))
         # initial joint velocity
         k = int(rng.integers(29))
-        vp, vm = prob["v0"].copy(), prob["v0"].copy()
-        vp[6 + k, e] += h
-        vm[6 + k, e] -= h
-        fd = (oracle_loss(oracle, prob, e, v0=vp) - oracle_loss(oracle, prob, e, v0=vm)) / (2 * h)
-        errs.append(abs(r64["grad_qvel0"][6 + k, e] - fd) / max(abs(fd), 1e-3))
-    errs = np.array(errs)
+
+        def fv(x, k=k):
+            v = prob["v0"].copy()
+            v[6 + k, e] += x
+            return oracle_loss(oracle, prob, e, v0=v)
+        check(r64["grad_qvel0"][6 + k, e], fv)
+    return np.array(errs)
+
+
+def test_fp64_gradients_match_central_differences(prob, r64, oracle):
+    """All 16 envs of the FD sample."""
+    errs = fd_errors(prob, r64, oracle, range(NENV))
     print(f"FD check: {len(errs)} entries, max rel err {errs.max():.2e}, median {np.median(errs):.2e}")
     assert np.median(errs) < 1e-6
+    assert errs.max() < 1e-4
+
+
+def switches(prob, oracle, e):
+    """Which switches the oracle trajectory of env e crosses."""
+    from oracle import EnvParams
+    cfg = oracle.config(dt=2e-3)
+    q = np.ascontiguousarray(prob["q0"][:, e], dtype=np.float64)
+    v = np.ascontiguousarray(prob["v0"][:, e], dtype=np.float64)
+    an = np.ascontiguousarray(prob["a0"][:, e], dtype=np.float64)
+    ep = EnvParams(1.0, 0.0, prob["kp"][e], prob["kd"][e])
+    dp = C.POINTER(C.c_double)
+    rng = np.asarray(M.jnt_range)
+    seen = set()
+    free0 = an >= 1e29
+    for t in range(H):
+        a_prev = an.copy()
+        u = np.ascontiguousarray(prob["tg"][t, :, e], dtype=np.float64)
+        oracle.lib.g1o_step(C.byref(cfg), C.byref(ep), q.ctypes.data_as(dp), v.ctypes.data_as(dp),
+                            u.ctypes.data_as(dp), an.ctypes.data_as(dp), 1, None, None, None)
+        if np.any(free0 & (an < 1e29)):
+            seen.add("touchdown")
+        stuck = (a_prev < 1e29) & (an < 1e29)
+        if np.any(np.abs(an - a_prev)[stuck] > 1e-9):
+            seen.add("slip")
+        if np.any(q[7:] < rng[:, 0]) or np.any(q[7:] > rng[:, 1]):
+            seen.add("limit")
+    return seen
+
+
+@pytest.mark.parametrize("kind,switch", [("touchdown", "touchdown"), ("slip", "slip"), ("limits", "limit")])
+def test_fd_across_switches(golden_host, oracle, kind, switch):
+    """Trajectories through touchdown, slip and soft-limit switches: the
+    adjoint is the derivative of the loss along the branches taken."""
+    prob = problem(golden_host, n=NENV, seed=21, kind=kind)
+    crossed = [e for e in range(NENV) if switch in switches(prob, oracle, e)]
+    assert len(crossed) >= NENV // 2, (kind, crossed)
+    r = run(prob, torch.float64)
+    for e in range(4):
+        ref = oracle_loss(oracle, prob, e)
+        assert abs(r["loss"][e] - ref) <= 1e-6 * abs(ref), (kind, e, r["loss"][e], ref)
+    straddled = []
+    errs = fd_errors(prob, r, oracle, crossed[:8], seed=7, straddled=straddled)
+    print(f"{kind}: {len(crossed)} of {NENV} envs cross it; FD check {len(errs)} entries, max rel err "
+          f"{errs.max():.2e}, median {np.median(errs):.2e}; {sum(straddled)} stencils straddled a switch")
+    assert sum(straddled) <= len(errs) // 10
+    assert np.median(errs) < 1e-5
     assert errs.max() < 1e-4
 
 

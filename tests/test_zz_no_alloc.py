@@ -83,7 +83,7 @@ def test_noalloc_rejects_problems_beyond_the_fixed_workspace(golden_host):
     cap = L.g1b_adjoint_noalloc_capacity()
     assert cap == 1 << 21
     H, ckpt = 64, 8
-    per_env = (H // ckpt + 1) * 87 + ckpt * 87 + 87 + 120
+    per_env = A.scratch_size(1, H, ckpt)  # (H / C + 1 + C) * 87 floats per env
     n = cap // per_env + 1  # one env too many
     x = inputs(golden_host, 2, H, 3)
     cfg = _lib.default_config(dt=2e-3)
