@@ -414,8 +414,27 @@ def adjoint_bench(device, stream, steps, warmup, world, n=ADJ_ENVS, horizon=ADJ_
         t, r = one()
         times.append(t)
     ms = max_over_ranks(statistics.mean(times), world, device)
+    # the plain step on the same envs for the same horizon (H substeps, one launch), for the cost ratio
+    from g1sim_b200 import _lib
+    from g1sim_b200 import g1sim as G
+    pq, pv, pa, pc = qp.clone(), qv.clone(), an.clone(), tg[0].contiguous()
+    cfg = _lib.default_config(dt=DT)
+    with torch.cuda.stream(stream):
+        G.step(pq, pv, pa, pc, H, config=cfg, kp_scale=kp, kd_scale=kd)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(5):
+            G.step(pq, pv, pa, pc, H, config=cfg, kp_scale=kp, kd_scale=kd)
+        e1.record(stream)
+    stream.synchronize()
+    plain_ms = e0.elapsed_time(e1) / 5
     return {"value": float(n) * H * world / (ms * 1e-3), "unit": "env-steps/s (horizon steps differentiated)",
-            "ms_per_call": ms, "config": {"envs": n, "horizon": H, "checkpoint": ADJ_C, "dt": DT,
+            "ms_per_call": ms,
+            "plain_step_same_envs": {"ms": plain_ms, "value": float(n) * H / (plain_ms * 1e-3),
+                                     "note": f"g1b_step, {n} envs x {H} substeps in one launch"},
+            "cost_vs_plain_same_envs": ms / plain_ms,
+            "config": {"envs": n, "horizon": H, "checkpoint": ADJ_C, "dt": DT,
                                          "decision_variables": f"targets {H}x29 + kp/kd scale per env"},
             "kernels": "adj_kernel<float, 32> (one launch: forward rollout with checkpoints, then per segment the "
                        "recomputed states and the reverse-mode product of each step; tape in shared memory)",

@@ -106,6 +106,15 @@ __device__ __forceinline__ void loss_grad(const XS& x, const R* up, size_t n, in
   for (int j = 0; j < adj::kNU; ++j) lam.put(7 + j, lam.get(7 + j) + R(2) * w * (x.get(7 + j) - up[(size_t)j * n + e]));
 }
 
+// One rolled-out substep.  The forward rollout and the segment
+// recomputation both call this one compiled copy, so that a recomputed state
+// equals the stored one bit for bit whatever the checkpoint interval.
+template <class R, int ENVS>
+__device__ __noinline__ void roll_step(adj::Base<R>& st, SCol<R, ENVS>& X, const GCol<R>& U, const adj::Par<R>& par,
+                                       const adj::Cfg<R>& cfg, adj::Tape<R, ENVS>& tp) {
+  adj::primal<true>(st, X, U, par, cfg, tp);
+}
+
 template <class R, int ENVS>
 constexpr size_t adj_smem() {
   return (size_t)(kTapeSlots + 2 * kState) * ENVS * sizeof(R);
@@ -140,7 +149,7 @@ __global__ void __launch_bounds__(ENVS) adj_kernel(AdjArgs<R> a) {
     }
     const R* ut = a.targets + (size_t)t * adj::kNU * n + e;
     const GCol<R> U{ut, n};
-    adj::primal<true>(st, X, U, par, a.cfg, tp);
+    roll_step<R, ENVS>(st, X, U, par, a.cfg, tp);
     const R dz = st.pos[2] - a.z_ref;
     R tr = R(0);
 #pragma unroll 1
@@ -170,7 +179,7 @@ __global__ void __launch_bounds__(ENVS) adj_kernel(AdjArgs<R> a) {
       x_store<R>(X, a.seg + (size_t)i * kState * n, n, e);
       if (i + 1 == len) break;
       const GCol<R> U{a.targets + (size_t)(t0 + i) * adj::kNU * n + e, n};
-      adj::primal<true>(st, X, U, par, a.cfg, tp);
+      roll_step<R, ENVS>(st, X, U, par, a.cfg, tp);
     }
 #pragma unroll 1
     for (int i = len - 1; i >= 0; --i) {
