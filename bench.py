@@ -62,8 +62,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
-    p.add_argument("--surrogate-steps", type=int, default=1000, help="training steps of the surrogate (-1: skip)")
-    p.add_argument("--part", default="all", choices=["all", "policy", "adjoint", "gemm"],
+    p.add_argument("--surrogate-steps", type=int, default=3000, help="training steps of the surrogate (-1: skip)")
+    p.add_argument("--part", default="all", choices=["all", "policy", "adjoint", "gemm", "surrogate"],
                    help="one sub-benchmark alone on --nenv envs (rows), one GPU (a small case for a profiler)")
     p.add_argument("--horizon", type=int, default=64, help="adjoint horizon with --part adjoint")
     return p.parse_args()
@@ -508,8 +508,11 @@ def surrogate_bench(device, train_steps, world):
     from g1sim_b200 import workloads
     w = workloads.randomized(nenv=SUR_ENVS, seed=7)
     st = {k: torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("qpos", "qvel", "anchor", "ctrl")}
-    st["contact_forces"] = torch.zeros(8, SUR_ENVS, device=device)
-    frac, err = S.rollout_with_fallback(sur, st, 50, bound=1e-3)
+    mu, dm = (torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("mu", "dmass"))
+    from g1sim_b200 import g1sim as G
+    G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 20, DECIM, config=_cfg(), seed=7, mu=mu, dmass=dm)
+    frac, err = S.rollout_with_fallback(sur, st, 50, bound=1e-3, mu=mu, dmass=dm)
+    ref = refinement_bench(sur, device)
     peak = measured_bf16_peak()
     return {"train_step_ms": step_ms, "train_tflops": train_tflops,
             "train_frac_of_bf16_peak": (train_tflops / peak) if peak else None,
@@ -518,9 +521,47 @@ def surrogate_bench(device, train_steps, world):
             "inference": {"value": SUR_BATCH / (fwd_ms * 1e-3), "unit": "env-steps/s (network forward only)"},
             "transitions": int(X.shape[0]), "generation_s": gen_s, "train_steps": train_steps,
             "loss_start": l0, "loss_end": l1,
-            "fallback_rollout": {"envs": SUR_ENVS, "steps": 50, "bound": 1e-3,
+            "fallback_rollout": {"envs": SUR_ENVS, "steps": 50, "bound": 1e-3, "start": "after 20 policy steps",
                                  "fraction_surrogate": frac, "one_step_error": err},
+            "refinement": ref,
             "gemm_status": S.gemm_status()}
+
+
+def _cfg():
+    from g1sim_b200 import _lib
+    return _lib.default_config(dt=DT)
+
+
+def refinement_bench(sur, device, n=4096, H=50, iters=10):
+    """Short-horizon refinement of the targets a policy chose for standing
+    envs (the drop test's stand + N(0, 0.1) targets, 200 substeps after the
+    drop): J = sum over H substeps of (z - 0.78)^2 + 0.1 |u - u0|^2 with u
+    held, `iters` normalised gradient steps per env, each judged by the exact
+    step.  Gradients from the surrogate rollout alone, from the surrogate
+    with fallback to the exact adjoint where its one-step error exceeds 5e-2,
+    and from the exact adjoint alone."""
+    import torch
+    from g1sim_b200 import surrogate as S
+    from g1sim_b200 import workloads
+    from g1sim_b200 import g1sim as G
+    w = workloads.drop_test(nenv=n, seed=9)
+    s = {k: torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("qpos", "qvel", "anchor", "ctrl")}
+    G.step(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], 200, config=_cfg())
+    u0 = s["ctrl"].clone()
+    J0 = S.exact_objective(s, u0, H, u0=u0, reg=0.1)
+    out = {"envs": n, "horizon_substeps": H, "iterations": iters, "objective_unrefined": float(J0.mean())}
+    for name, mode, bound in (("surrogate", "surrogate", None), ("surrogate_with_fallback", "surrogate", 5e-2),
+                              ("exact", "exact", None)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, J, frac = S.refine_targets(sur, s, u0, H=H, iters=iters, mode=mode, bound=bound)
+        torch.cuda.synchronize()
+        out[name] = {"objective": float(J.mean()), "envs_improved": float((J < J0).float().mean()),
+                     "seconds": time.perf_counter() - t0}
+        if mode == "surrogate":
+            out[name]["fraction_on_surrogate_gradient"] = frac
+            out[name]["bound"] = bound
+    return out
 
 
 def gemm_bench(device, rows, steps, warmup):
@@ -561,6 +602,8 @@ def part_only(args, local):
         init = {k: torch.tensor(w[k], dtype=torch.float32, device=device)
                 for k in ("qpos", "qvel", "anchor", "ctrl", "mu", "dmass")}
         r = policy_fused_bench(args.nenv, 0, device, stream, args.steps, args.warmup, 1, local, init)
+    elif args.part == "surrogate":
+        r = surrogate_bench(device, args.surrogate_steps, 1)
     elif args.part == "adjoint":
         r = adjoint_bench(device, stream, args.steps, args.warmup, 1, n=args.nenv, horizon=args.horizon)
     else:

@@ -98,8 +98,12 @@ def lib():
     L.g1b_sur_loss.argtypes = [C.c_int, C.c_int] + [_vp] * 8
     L.g1b_sur_adam.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _vp]
     L.g1b_sur_cast.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
-    L.g1b_sur_features.argtypes = [C.c_int] + [_vp] * 10
+    L.g1b_sur_features.argtypes = [C.c_int] + [_vp] * 12
+    L.g1b_sur_features_vjp.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
     L.g1b_sur_integrate.argtypes = [C.c_int, _vp, C.c_int, _vp, _vp, C.c_float, _vp, _vp, _vp]
+    L.g1b_sur_integrate_vjp.argtypes = [C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp, C.c_float, _vp, _vp, _vp,
+                                        C.c_int, _vp]
+    L.g1b_sur_seed.argtypes = [C.c_int, _vp, _vp, _vp]
     L.g1b_adjoint_scratch_size.argtypes = [C.c_int, C.POINTER(AdjointProblem), C.POINTER(C.c_size_t)]
     for name in ("g1b_adjoint", "g1b_adjoint_f64"):
         getattr(L, name).argtypes = [C.c_int, C.POINTER(Config), C.POINTER(AdjointProblem)] + [_vp] * 14

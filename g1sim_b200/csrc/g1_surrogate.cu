@@ -9,6 +9,7 @@
 
 #include "g1_host.h"
 #include "g1_mlp.cuh"
+#include "g1_surfeat.cuh"
 
 namespace g1b {
 #include "g1_gemm.cuh"
@@ -116,12 +117,25 @@ int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* s
   return launched("sur_cast_kernel");
 }
 
-int g1b_sur_features(int n, const float* qpos, const float* qvel, const float* ctrl, const float* cf,
-                     const float* mean, const float* istd, void* X, void* Xt, float* F, void* stream) {
-  if (n <= 0 || !qpos || !qvel || !ctrl || !mean || !istd || !X) return fail("sur_features: invalid arguments");
+int g1b_sur_features(int n, const float* qpos, const float* qvel, const float* anchor, const float* ctrl,
+                     const float* mu, const float* dmass, const float* mean, const float* istd, void* X, void* Xt,
+                     float* F, void* stream) {
+  if (n <= 0 || !qpos || !qvel || !anchor || !ctrl || !mean || !istd || !X)
+    return fail("sur_features: invalid arguments");
   sur_features_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
-      n, qpos, qvel, ctrl, cf, mean, istd, static_cast<__nv_bfloat16*>(X), static_cast<__nv_bfloat16*>(Xt), F);
+      n, qpos, qvel, anchor, ctrl, mu, dmass, mean, istd, static_cast<__nv_bfloat16*>(X),
+      static_cast<__nv_bfloat16*>(Xt), F);
   return launched("sur_features_kernel");
+}
+
+int g1b_sur_features_vjp(int n, const float* qpos, const float* qvel, const float* anchor, const float* istd,
+                         const float* dX, int ld, float* qpos_b, float* qvel_b, float* anchor_b, float* ctrl_b,
+                         void* stream) {
+  if (n <= 0 || !qpos || !qvel || !anchor || !istd || !dX || ld < kSurFeat || !qpos_b || !qvel_b || !ctrl_b)
+    return fail("sur_features_vjp: invalid arguments");
+  sur_feat_vjp_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, qpos, qvel, anchor, istd, dX, ld, qpos_b, qvel_b, anchor_b, ctrl_b);
+  return launched("sur_feat_vjp_kernel");
 }
 
 int g1b_sur_integrate(int n, const float* Y, int ldy, const float* omean, const float* ostd, float dt, float* qpos,
@@ -130,6 +144,23 @@ int g1b_sur_integrate(int n, const float* Y, int ldy, const float* omean, const 
   sur_integrate_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(n, Y, ldy, omean, ostd, dt,
                                                                                        qpos, qvel);
   return launched("sur_integrate_kernel");
+}
+
+int g1b_sur_integrate_vjp(int n, const float* qpos, const float* qvel, const float* Y, int ldy, const float* omean,
+                          const float* ostd, float dt, float* lam_qpos, float* lam_qvel, float* dY, int ldd,
+                          void* stream) {
+  if (n <= 0 || !qpos || !qvel || !Y || ldy < kNV || !omean || !ostd || !lam_qpos || !lam_qvel || !dY || ldd < kNV)
+    return fail("sur_integrate_vjp: invalid arguments");
+  sur_integrate_vjp_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, qpos, qvel, Y, ldy, omean, ostd, dt, lam_qpos, lam_qvel, dY, ldd);
+  return launched("sur_integrate_vjp_kernel");
+}
+
+int g1b_sur_seed(int total, const float* dY, void* dZ, void* stream) {
+  if (total <= 0 || !dY || !dZ) return fail("sur_seed: invalid arguments");
+  sur_seed_kernel<<<grid_1d((size_t)total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      total, dY, static_cast<__nv_bfloat16*>(dZ));
+  return launched("sur_seed_kernel");
 }
 
 }  // extern "C"

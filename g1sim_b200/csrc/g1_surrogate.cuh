@@ -1,17 +1,19 @@
 // g1_surrogate.cuh -- kernels of the learned one-step dynamics surrogate
 // (included by g1_kernels.cu inside namespace g1b, after g1_gemm.cuh).
 //
-// The surrogate is an MLP 128 -> 512 -> 512 -> 512 -> 512 -> 64 with SiLU on
+// The surrogate is an MLP 192 -> 512 -> 512 -> 512 -> 512 -> 64 with SiLU on
 // the hidden layers, over a normalised feature vector of the state and the
-// PD targets, predicting the normalised generalised acceleration of the step
-// (the state delta is dt * qacc for qvel, and qpos follows by the step's own
-// semi-implicit Euler).  Its matrix products run on gemm_bf16_kernel
+// PD targets (g1_surfeat.cuh), predicting the normalised generalised
+// acceleration of the step (the state delta is dt * qacc for qvel, and qpos
+// follows by the step's own semi-implicit Euler).  The feature and update
+// kernels also have their vector-Jacobian products, so that a loss can be
+// differentiated through a surrogate rollout.  Its matrix products run on gemm_bf16_kernel
 // (tcgen05); the element-wise parts of the forward and backward passes, the
 // loss, Adam and the feature extraction are the kernels below.
 
-constexpr int kSurIn = 128;    // padded input features (109 used)
-constexpr int kSurOut = 64;    // padded outputs (35 used: qacc)
-constexpr int kSurFeat = 109;  // q 29, qd 29, z 1, rot6 6, v body 3, w body 3, contact flags 8, targets 29, 1
+using sur::kSurFeat;
+using sur::kSurIn;
+constexpr int kSurOut = 64;  // padded outputs (35 used: qacc)
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
@@ -145,82 +147,135 @@ __global__ void sur_cast_kernel(int rows, int cols, const float* __restrict__ W,
   }
 }
 
-// Feature vector of env e (raw, before normalisation): joint angles and
-// rates, base height, the first two columns of the base rotation, base
-// linear and angular velocity in the body frame, contact flags (normal force
-// > 0 per sphere), PD targets, and a constant 1.
-__device__ __forceinline__ void sur_features_raw(const float* qpos, const float* qvel, const float* ctrl,
-                                                 const float* cf, size_t n, int e, float* f) {
-  int k = 0;
-  for (int j = 0; j < 29; ++j) f[k++] = qpos[(size_t)(7 + j) * n + e];
-  for (int j = 0; j < 29; ++j) f[k++] = qvel[(size_t)(6 + j) * n + e];
-  f[k++] = qpos[2 * n + e];
-  const float qw = qpos[3 * n + e], qx = qpos[4 * n + e], qy = qpos[5 * n + e], qz = qpos[6 * n + e];
-  const float R[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz),     2 * (qx * qz + qw * qy),
-                      2 * (qx * qy + qw * qz),     1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
-                      2 * (qx * qz - qw * qy),     2 * (qy * qz + qw * qx),     1 - 2 * (qx * qx + qy * qy)};
-  f[k++] = R[0];
-  f[k++] = R[3];
-  f[k++] = R[6];
-  f[k++] = R[1];
-  f[k++] = R[4];
-  f[k++] = R[7];
-  const float vw[3] = {qvel[e], qvel[n + e], qvel[2 * n + e]};
-  for (int i = 0; i < 3; ++i) f[k++] = R[i] * vw[0] + R[3 + i] * vw[1] + R[6 + i] * vw[2];  // R^T v
-  for (int i = 0; i < 3; ++i) f[k++] = qvel[(size_t)(3 + i) * n + e];
-  for (int i = 0; i < 8; ++i) f[k++] = cf ? (cf[(size_t)i * n + e] > 0.0f ? 1.0f : 0.0f) : 0.0f;
-  for (int j = 0; j < 29; ++j) f[k++] = ctrl[(size_t)j * n + e];
-  f[k++] = 1.0f;
-}
+// One env's state and targets as seen by the feature and update functions:
+// the 87 state entries (qpos, qvel, anchors) over the SoA arrays.
+struct SoAState {
+  float* qpos;
+  float* qvel;
+  const float* anchor;
+  size_t n;
+  int e;
+  __device__ __forceinline__ float get(int k) const {
+    return k < kNQ ? qpos[(size_t)k * n + e]
+                   : (k < kNQ + kNV ? qvel[(size_t)(k - kNQ) * n + e] : anchor[(size_t)(k - kNQ - kNV) * n + e]);
+  }
+  __device__ __forceinline__ void put(int k, float v) {
+    if (k < kNQ)
+      qpos[(size_t)k * n + e] = v;
+    else if (k < kNQ + kNV)
+      qvel[(size_t)(k - kNQ) * n + e] = v;
+  }
+};
+struct SoACol {
+  const float* p;
+  size_t n;
+  int e;
+  __device__ __forceinline__ float get(int k) const { return p[(size_t)k * n + e]; }
+};
+// accumulating column of a SoA array (adjoints)
+struct SoAAdd {
+  float* p;
+  size_t n;
+  int e;
+  __device__ __forceinline__ void add(int k, float v) { p[(size_t)k * n + e] += v; }
+};
+// adjoint of the 87 state entries over (qpos, qvel, anchor) SoA arrays; the
+// anchors' adjoint is dropped when anchor is null
+struct SoAStateAdd {
+  float* qpos;
+  float* qvel;
+  float* anchor;
+  size_t n;
+  int e;
+  __device__ __forceinline__ void add(int k, float v) {
+    if (k < kNQ)
+      qpos[(size_t)k * n + e] += v;
+    else if (k < kNQ + kNV)
+      qvel[(size_t)(k - kNQ) * n + e] += v;
+    else if (anchor)
+      anchor[(size_t)(k - kNQ - kNV) * n + e] += v;
+  }
+  __device__ __forceinline__ float get(int k) const {
+    return k < kNQ ? qpos[(size_t)k * n + e] : qvel[(size_t)(k - kNQ) * n + e];
+  }
+  __device__ __forceinline__ void put(int k, float v) {
+    if (k < kNQ)
+      qpos[(size_t)k * n + e] = v;
+    else if (k < kNQ + kNV)
+      qvel[(size_t)(k - kNQ) * n + e] = v;
+  }
+};
 
-// X[e][:] = BF16((f - mean) * istd), padded with zeros to 128; Xt the
-// transpose (nullable); raw features to F (FP32 [n][128], nullable).
-__global__ void sur_features_kernel(int n, const float* qpos, const float* qvel, const float* ctrl, const float* cf,
-                                    const float* __restrict__ mean, const float* __restrict__ istd,
-                                    __nv_bfloat16* X, __nv_bfloat16* Xt, float* F) {
+// X[e][:] = BF16((f - mean) * istd), padded with zeros to kSurIn; Xt the
+// transpose (nullable); raw features to F (FP32 [n][kSurIn], nullable).
+// mu, dmass: per-env friction and base-mass offset (nullable: 1, 0).
+__global__ void sur_features_kernel(int n, const float* qpos, const float* qvel, const float* anchor, const float* ctrl,
+                                    const float* mu, const float* dmass, const float* __restrict__ mean,
+                                    const float* __restrict__ istd, __nv_bfloat16* X, __nv_bfloat16* Xt, float* F) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   float f[kSurFeat];
-  sur_features_raw(qpos, qvel, ctrl, cf, (size_t)n, e, f);
+  const SoAState x{const_cast<float*>(qpos), const_cast<float*>(qvel), anchor, (size_t)n, e};
+  sur::features<float>(x, SoACol{ctrl, (size_t)n, e}, mu ? mu[e] : (float)g1m_contact_mu, dmass ? dmass[e] : 0.0f, f);
   for (int k = 0; k < kSurIn; ++k) {
     const float raw = k < kSurFeat ? f[k] : 0.0f;
     if (F) F[(size_t)e * kSurIn + k] = raw;
-    const float x = k < kSurFeat ? (raw - mean[k]) * istd[k] : 0.0f;
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    const float xv = k < kSurFeat ? (raw - mean[k]) * istd[k] : 0.0f;
+    const __nv_bfloat16 h = __float2bfloat16_rn(xv);
     X[(size_t)e * kSurIn + k] = h;
     if (Xt) Xt[(size_t)k * n + e] = h;
   }
 }
 
+// Adjoint of the features: dX [n][ld] is the adjoint of the normalised
+// inputs; the state adjoints (qpos_b [36][n], qvel_b [35][n], anchor_b
+// [16][n] nullable) and the targets' (ctrl_b [29][n]) are accumulated.
+__global__ void sur_feat_vjp_kernel(int n, const float* qpos, const float* qvel, const float* anchor,
+                                    const float* __restrict__ istd, const float* __restrict__ dX, int ld,
+                                    float* qpos_b, float* qvel_b, float* anchor_b, float* ctrl_b) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  float fb[kSurFeat];
+  for (int k = 0; k < kSurFeat; ++k) fb[k] = dX[(size_t)e * ld + k] * istd[k];
+  const SoAState x{const_cast<float*>(qpos), const_cast<float*>(qvel), anchor, (size_t)n, e};
+  SoAStateAdd xb{qpos_b, qvel_b, anchor_b, (size_t)n, e};
+  SoAAdd ub{ctrl_b, (size_t)n, e};
+  sur::features_vjp<float>(x, fb, xb, ub);
+}
+
 // One surrogate step in place: qacc = Y[e][0:35] * ostd + omean, then the
-// step's semi-implicit Euler (qvel += dt qacc; qpos from the new qvel, the
-// base quaternion by q (x) exp(w dt / 2)).  Anchors are left free.
+// step's semi-implicit Euler (g1_surfeat.cuh).  Anchors are not touched.
 __global__ void sur_integrate_kernel(int n, const float* __restrict__ Y, int ldy, const float* __restrict__ omean,
                                      const float* __restrict__ ostd, float dt, float* qpos, float* qvel) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
-  const size_t sn = (size_t)n;
-  for (int i = 0; i < kNV; ++i) {
-    const float a = Y[(size_t)e * ldy + i] * ostd[i] + omean[i];
-    qvel[i * sn + e] += dt * a;
-  }
-  for (int i = 0; i < 3; ++i) qpos[i * sn + e] += dt * qvel[i * sn + e];
-  const float wx = qvel[3 * sn + e], wy = qvel[4 * sn + e], wz = qvel[5 * sn + e];
-  const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
-  const float ang = wn * dt;
-  if (ang >= 1e-12f) {
-    const float s = sinf(0.5f * ang) / wn, c = cosf(0.5f * ang);
-    const float dx = s * wx, dy = s * wy, dz = s * wz;
-    const float aw = qpos[3 * sn + e], ax = qpos[4 * sn + e], ay = qpos[5 * sn + e], az = qpos[6 * sn + e];
-    float rw = aw * c - ax * dx - ay * dy - az * dz;
-    float rx = aw * dx + ax * c + ay * dz - az * dy;
-    float ry = aw * dy - ax * dz + ay * c + az * dx;
-    float rz = aw * dz + ax * dy - ay * dx + az * c;
-    const float inv = 1.0f / sqrtf(rw * rw + rx * rx + ry * ry + rz * rz);
-    qpos[3 * sn + e] = rw * inv;
-    qpos[4 * sn + e] = rx * inv;
-    qpos[5 * sn + e] = ry * inv;
-    qpos[6 * sn + e] = rz * inv;
-  }
-  for (int h = 0; h < 29; ++h) qpos[(7 + h) * sn + e] += dt * qvel[(6 + h) * sn + e];
+  float a[kNV];
+  for (int i = 0; i < kNV; ++i) a[i] = Y[(size_t)e * ldy + i] * ostd[i] + omean[i];
+  SoAState x{qpos, qvel, nullptr, (size_t)n, e};
+  sur::integrate<float>(x, a, dt);
+}
+
+// Reverse of sur_integrate at the state before the update (qpos, qvel):
+// lam_qpos [36][n], lam_qvel [35][n] hold the adjoint of the updated state
+// and are replaced by the adjoint of the state through the update; dY
+// [n][ldd] (FP32) gets the adjoint of the normalised network output (zero
+// past the 35 used columns).
+__global__ void sur_integrate_vjp_kernel(int n, const float* qpos, const float* qvel, const float* __restrict__ Y,
+                                         int ldy, const float* __restrict__ omean, const float* __restrict__ ostd,
+                                         float dt, float* lam_qpos, float* lam_qvel, float* dY, int ldd) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  float a[kNV], ab[kNV];
+  for (int i = 0; i < kNV; ++i) a[i] = Y[(size_t)e * ldy + i] * ostd[i] + omean[i];
+  const SoAState x{const_cast<float*>(qpos), const_cast<float*>(qvel), nullptr, (size_t)n, e};
+  SoAStateAdd lam{lam_qpos, lam_qvel, nullptr, (size_t)n, e};
+  sur::integrate_vjp<float>(x, a, dt, lam, ab);
+  for (int i = 0; i < ldd; ++i) dY[(size_t)e * ldd + i] = i < kNV ? ab[i] * ostd[i] : 0.0f;
+}
+
+// BF16 copy of an FP32 [B][D] adjoint (the seed of the network's input
+// gradient chain).
+__global__ void sur_seed_kernel(int total, const float* __restrict__ dY, __nv_bfloat16* dZ) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+    dZ[i] = __float2bfloat16_rn(dY[i]);
 }

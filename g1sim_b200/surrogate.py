@@ -1,12 +1,13 @@
 """Learned one-step dynamics surrogate of the G1 step.
 
-An MLP 128 -> 4 x 512 (SiLU) -> 64 over a normalised feature vector of the
+An MLP 192 -> 4 x 512 (SiLU) -> 64 over a normalised feature vector of the
 state and the PD targets (joint angles and rates, base height, the first two
-columns of the base rotation, body-frame base velocities, foot-sphere
-contact flags, targets; 109 used, padded to 128) predicting the normalised
-generalised acceleration of the step (35 used, padded to 64).  The state
-delta is dt * qacc for qvel; qpos follows by the step's semi-implicit Euler
-(sur_integrate_kernel).
+columns of the base rotation, body-frame base velocities, per foot sphere
+its penetration depth, contact flag, offset from its anchor and world
+velocity, targets, friction, base-mass offset; 159 used, padded to 192;
+csrc/g1_surfeat.cuh) predicting the normalised generalised acceleration of
+the step (35 used, padded to 64).  The state delta is dt * qacc for qvel;
+qpos follows by the step's semi-implicit Euler (sur_integrate_kernel).
 
 Training runs on the library's own kernels: BF16 tcgen05 GEMMs with FP32
 accumulation (g1b_gemm_bf16) for the forward pass, the input-gradient and
@@ -18,6 +19,16 @@ The exact step stays the judge: `rollout_with_fallback` advances each env
 with the surrogate only where its one-step error against the exact step is
 within a bound (1e-3, relative per state component) and with the exact step
 elsewhere.
+
+What the surrogate is for is its gradient: `rollout_grad` differentiates a
+short-horizon objective through a surrogate rollout (features, network and
+state update each have a vector-Jacobian product kernel), which is smooth
+across the contact switches where the exact step's derivative jumps.
+`refine_targets` uses it for short-horizon refinement of the PD targets a
+policy chose, with the exact step as the judge of every update (an update
+that does not lower the exact objective is rejected and its step size
+halved) and as the fallback (envs whose surrogate one-step error exceeds the
+bound take the exact adjoint's gradient).
 """
 import ctypes as C
 
@@ -28,8 +39,8 @@ from . import _lib
 from . import g1sim as G
 from .model import g1_model_data as M
 
-DIMS = [128, 512, 512, 512, 512, 64]
-NFEAT, NOUT = 109, 35
+DIMS = [192, 512, 512, 512, 512, 64]
+NFEAT, NOUT, NIN = 159, 35, 192
 
 
 def _p(t):
@@ -80,8 +91,8 @@ class Surrogate:
         self.gW = [torch.zeros(max(w.shape[0], 128), w.shape[1], device=device) for w in self.W]
         self.gb = [torch.zeros_like(b) for b in self.b]
         self.step_n = 0
-        self.in_mean = torch.zeros(128, device=device)
-        self.in_istd = torch.ones(128, device=device)
+        self.in_mean = torch.zeros(NIN, device=device)
+        self.in_istd = torch.ones(NIN, device=device)
         self.out_mean = torch.zeros(64, device=device)
         self.out_std = torch.ones(64, device=device)
         self.out_w = torch.zeros(64, device=device)
@@ -102,17 +113,21 @@ class Surrogate:
                 H=[None] + [torch.empty(B, DIMS[i], dtype=bf, device=d) for i in range(1, 5)],
                 Ht=[None] + [torch.empty(DIMS[i], B, dtype=bf, device=d) for i in range(1, 5)],
                 dH=torch.empty(B, 512, device=d),
-                dX=torch.empty(B, 128, device=d),
+                dX=torch.empty(B, NIN, device=d),
+                dY=torch.zeros(B, 64, device=d),
+                db=torch.zeros(512, device=d),
                 dZ=torch.empty(B, 512, dtype=bf, device=d),
                 dZt=torch.zeros(512, B, dtype=bf, device=d),
                 loss=torch.zeros(1, device=d))
         return self._ws[B]
 
-    def features(self, qpos, qvel, ctrl, cf, X, Xt=None, raw=None):
+    def features(self, qpos, qvel, anchor, ctrl, X, Xt=None, raw=None, mu=None, dmass=None):
+        """Normalised BF16 features X [n, 192] of the SoA state (Xt [192, n]
+        and the raw FP32 features raw [n, 192] optional)."""
         n = qpos.shape[1]
-        _lib.check(_lib.lib().g1b_sur_features(n, _p(qpos), _p(qvel), _p(ctrl), _p(cf), _p(self.in_mean),
-                                                _p(self.in_istd), _p(X), _p(Xt), _p(raw), _st(self.device)),
-                   "sur_features")
+        _lib.check(_lib.lib().g1b_sur_features(n, _p(qpos), _p(qvel), _p(anchor), _p(ctrl), _p(mu), _p(dmass),
+                                                _p(self.in_mean), _p(self.in_istd), _p(X), _p(Xt), _p(raw),
+                                                _st(self.device)), "sur_features")
 
     def forward(self, X, keep=False):
         """Normalised prediction Y [B, 64] (FP32) for BF16 inputs X [B, 128]."""
@@ -165,6 +180,28 @@ class Surrogate:
     def dX(self, B):
         return self._work(B)["dX"]
 
+    def input_grad(self, X, dY):
+        """d / d X of <dY, Y> for the last forward(X, keep=True): dY [B, 64]
+        FP32 adjoint of the normalised output; returns dX [B, 192] (FP32).
+        The network's backward products without the weight gradients."""
+        B = X.shape[0]
+        w = self._work(B)
+        L = _lib.lib()
+        st = _st(self.device)
+        dZ = w["dZ"]
+        _lib.check(L.g1b_sur_seed(B * 64, _p(dY), _p(dZ), st), "sur_seed")
+        for i in range(4, -1, -1):
+            Din, Dout = DIMS[i], DIMS[i + 1]
+            dz = dZ.view(-1)[:B * Dout].view(B, Dout)
+            if i > 0:
+                dh = w["dH"].view(-1)[:B * Din].view(B, Din)
+                gemm(dz, self.Wt[i], dh)
+                _lib.check(L.g1b_sur_act_bwd(B, Din, _p(dh), _p(w["Z"][i]), _p(dZ), _p(w["dZt"]), _p(w["db"]), st),
+                           "sur_act_bwd")
+            else:
+                gemm(dz, self.Wt[0], w["dX"])
+        return w["dX"]
+
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
         self.step_n += 1
         L = _lib.lib()
@@ -193,7 +230,7 @@ class Surrogate:
 def generate_transitions(sur, n_envs, n_steps, device, dt=2e-3, decim=10, seed=0):
     """Transitions of the randomised workload's simulator (targets stand +
     U(-0.3, 0.3) x range redrawn every `decim` steps, friction / base mass
-    randomised, reset below 0.3 m): raw features F [N, 128] and qacc
+    randomised, reset below 0.3 m): raw features F [N, 192] and qacc
     targets [N, 35] for N = n_envs * n_steps."""
     from . import workloads
     w = workloads.randomized(nenv=n_envs, seed=seed)
@@ -207,16 +244,16 @@ def generate_transitions(sur, n_envs, n_steps, device, dt=2e-3, decim=10, seed=0
     span = (rg[:, 1] - rg[:, 0])[:, None]
     cfg = _lib.default_config(dt=dt)
     N = n_envs * n_steps
-    F = torch.empty(N, 128, **f32)
+    F = torch.empty(N, NIN, **f32)
     A = torch.empty(N, 35, **f32)
-    Xtmp = torch.empty(n_envs, 128, dtype=torch.bfloat16, device=device)
+    Xtmp = torch.empty(n_envs, NIN, dtype=torch.bfloat16, device=device)
     done = torch.zeros(n_envs, dtype=torch.uint8, device=device)
     for t in range(n_steps):
         if t % decim == 0:
             u = torch.rand(29, n_envs, generator=rng, device=device)
             s["ctrl"].copy_(stand + (2 * u - 1) * 0.3 * span)
         rows = slice(t * n_envs, (t + 1) * n_envs)
-        sur.features(s["qpos"], s["qvel"], s["ctrl"], cf, Xtmp, None, F[rows])
+        sur.features(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], Xtmp, None, F[rows], mu=mu, dmass=dm)
         v0 = s["qvel"].clone()
         G.step(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], 1, config=cfg, mu=mu, dmass=dm, foot_pos=fp,
                foot_vel=fv, contact_forces=cf)
@@ -246,7 +283,7 @@ def fit_normalisation(sur, F, A):
 
 
 def normalise(sur, F, A=None):
-    """BF16 inputs X [N, 128] (and FP32 targets T [N, 64]) from raw features."""
+    """BF16 inputs X [N, 192] (and FP32 targets T [N, 64]) from raw features."""
     X = ((F - sur.in_mean) * sur.in_istd).to(torch.bfloat16)
     if A is None:
         return X
@@ -273,18 +310,30 @@ def train(sur, F, A, steps, batch=65536, lr=1e-3, seed=0, log_every=0):
     return hist
 
 
-def predict_next(sur, s, dt):
+def _pad_rows(n):
+    return n + (-n) % 128
+
+
+def predict_next(sur, s, dt, mu=None, dmass=None):
     """Surrogate one-step prediction from the state dict s (copies)."""
     n = s["qpos"].shape[1]
-    X = torch.empty(n, 128, dtype=torch.bfloat16, device=sur.device)
-    sur.features(s["qpos"], s["qvel"], s["ctrl"], s["contact_forces"], X)
-    pad = (-n) % 128
-    if pad:
-        X = torch.cat([X, torch.zeros(pad, 128, dtype=torch.bfloat16, device=sur.device)])
+    X = torch.zeros(_pad_rows(n), NIN, dtype=torch.bfloat16, device=sur.device)
+    sur.features(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], X, mu=mu, dmass=dmass)
     Y = sur.forward(X)[:n]
     q, v = s["qpos"].clone(), s["qvel"].clone()
     sur.integrate(Y.contiguous(), q, v, dt)
     return q, v
+
+
+def one_step_error(sur, s, dt=2e-3, mu=None, dmass=None):
+    """Per-env one-step error of the surrogate against the exact step from
+    state s: max over qpos and qvel components of |x_sur - x| / max(|x|, 1)."""
+    qs, vs = predict_next(sur, s, dt, mu, dmass)
+    ex = {k: s[k].clone() for k in ("qpos", "qvel", "anchor")}
+    G.step(ex["qpos"], ex["qvel"], ex["anchor"], s["ctrl"], 1, config=_lib.default_config(dt=dt), mu=mu, dmass=dmass)
+    eq = ((qs - ex["qpos"]).abs() / ex["qpos"].abs().clamp_min(1.0)).amax(0)
+    ev = ((vs - ex["qvel"]).abs() / ex["qvel"].abs().clamp_min(1.0)).amax(0)
+    return torch.maximum(eq, ev), qs, vs, ex
 
 
 def rollout_with_fallback(sur, s, steps, dt=2e-3, bound=1e-3, mu=None, dmass=None):
@@ -292,18 +341,11 @@ def rollout_with_fallback(sur, s, steps, dt=2e-3, bound=1e-3, mu=None, dmass=Non
     error against the exact step is <= bound (relative per component of
     qpos and qvel), else with the exact step.  Returns (fraction of env-steps
     taken by the surrogate, statistics of the one-step error: median, 90th
-    percentile and the fractions of env-steps within 1e-2 and 1e-1)."""
-    cfg = _lib.default_config(dt=dt)
+    percentile and the fractions of env-steps within 1e-3, 1e-2 and 1e-1)."""
     used, errs = 0, []
     n = s["qpos"].shape[1]
     for _ in range(steps):
-        qs, vs = predict_next(sur, s, dt)
-        ex = {k: s[k].clone() for k in ("qpos", "qvel", "anchor")}
-        G.step(ex["qpos"], ex["qvel"], ex["anchor"], s["ctrl"], 1, config=cfg, mu=mu, dmass=dmass,
-               contact_forces=s["contact_forces"])
-        eq = ((qs - ex["qpos"]).abs() / ex["qpos"].abs().clamp_min(1.0)).amax(0)
-        ev = ((vs - ex["qvel"]).abs() / ex["qvel"].abs().clamp_min(1.0)).amax(0)
-        err = torch.maximum(eq, ev)
+        err, qs, vs, ex = one_step_error(sur, s, dt, mu, dmass)
         ok = err <= bound
         used += int(ok.sum().item())
         errs.append(err)
@@ -312,6 +354,117 @@ def rollout_with_fallback(sur, s, steps, dt=2e-3, bound=1e-3, mu=None, dmass=Non
         s["anchor"].copy_(ex["anchor"])
     e = torch.cat(errs)
     stats = {"median": float(e.median().item()), "p90": float(torch.quantile(e[:1 << 24].float(), 0.9).item()),
+             "within_1e-3": float((e <= 1e-3).float().mean().item()),
              "within_1e-2": float((e <= 1e-2).float().mean().item()),
              "within_1e-1": float((e <= 1e-1).float().mean().item())}
     return used / float(n * steps), stats
+
+
+# ---------------------------------------------- gradients and refinement
+# Short-horizon objective of a target vector u held for H substeps from the
+# state s (the adjoint workload's height term plus a proximity term to the
+# policy's targets u0):  J(u) = sum_{t=1..H} (z_t - z_ref)^2 + reg |u - u0|^2.
+
+def exact_objective(s, u, H, z_ref=0.78, dt=2e-3, mu=None, dmass=None, u0=None, reg=0.0):
+    """J per env with the exact step (the judge).  s is not modified."""
+    x = {k: s[k].clone() for k in ("qpos", "qvel", "anchor")}
+    cfg = _lib.default_config(dt=dt)
+    J = torch.zeros(u.shape[1], device=u.device)
+    for _ in range(H):
+        G.step(x["qpos"], x["qvel"], x["anchor"], u, 1, config=cfg, mu=mu, dmass=dmass)
+        J += (x["qpos"][2] - z_ref) ** 2
+    if u0 is not None and reg > 0:
+        J += reg * ((u - u0) ** 2).sum(0)
+    return J
+
+
+def exact_grad(s, u, H, z_ref=0.78, dt=2e-3, u0=None, reg=0.0):
+    """dJ/du by the exact step's adjoint (g1b_adjoint, targets held: the
+    per-step target gradients summed); friction 1, no mass offset."""
+    from . import adjoint as A
+    n = u.shape[1]
+    tg = u[None].expand(H, 29, n).contiguous()
+    r = A.horizon_adjoint(tg, None, None, s["qpos"].contiguous(), s["qvel"].contiguous(), s["anchor"].contiguous(),
+                          checkpoint=min(8, H), z_ref=z_ref, w_track=0.0, config=_lib.default_config(dt=dt))
+    g = r["grad_targets"].sum(0)
+    if u0 is not None and reg > 0:
+        g = g + 2 * reg * (u - u0)
+    return g
+
+
+def rollout_grad(sur, s, u, H, z_ref=0.78, dt=2e-3, mu=None, dmass=None, u0=None, reg=0.0):
+    """(J_sur, dJ_sur/du) per env through an H-step surrogate rollout from
+    the exact state s (anchors held at their values in s), by
+    backpropagation through the feature, network and update kernels."""
+    L = _lib.lib()
+    st = _st(sur.device)
+    n = u.shape[1]
+    B = _pad_rows(n)
+    X = torch.zeros(B, NIN, dtype=torch.bfloat16, device=sur.device)
+    qs, vs, Ys = [s["qpos"].clone()], [s["qvel"].clone()], []
+    an = s["anchor"]
+    J = torch.zeros(n, device=u.device)
+    for _ in range(H):  # forward: keep the states and the network outputs
+        q, v = qs[-1].clone(), vs[-1].clone()
+        sur.features(q, v, an, u, X, mu=mu, dmass=dmass)
+        Y = sur.forward(X)[:n].clone()
+        sur.integrate(Y, q, v, dt)
+        Ys.append(Y)
+        qs.append(q)
+        vs.append(v)
+        J += (q[2] - z_ref) ** 2
+    lq = torch.zeros_like(qs[0])
+    lv = torch.zeros_like(vs[0])
+    lq[2] = 2 * (qs[H][2] - z_ref)
+    ub = torch.zeros_like(u)
+    dY = torch.zeros(B, 64, device=sur.device)
+    for t in range(H - 1, -1, -1):
+        _lib.check(L.g1b_sur_integrate_vjp(n, _p(qs[t]), _p(vs[t]), _p(Ys[t]), Ys[t].stride(0), _p(sur.out_mean),
+                                           _p(sur.out_std), dt, _p(lq), _p(lv), _p(dY), 64, st), "sur_integrate_vjp")
+        sur.features(qs[t], vs[t], an, u, X, mu=mu, dmass=dmass)
+        sur.forward(X, keep=True)
+        dX = sur.input_grad(X, dY)
+        _lib.check(L.g1b_sur_features_vjp(n, _p(qs[t]), _p(vs[t]), _p(an), _p(sur.in_istd), _p(dX), NIN, _p(lq),
+                                          _p(lv), None, _p(ub), st), "sur_features_vjp")
+        if t >= 1:
+            lq[2] += 2 * (qs[t][2] - z_ref)
+    if u0 is not None and reg > 0:
+        J = J + reg * ((u - u0) ** 2).sum(0)
+        ub = ub + 2 * reg * (u - u0)
+    return J, ub
+
+
+def refine_targets(sur, s, u0, H=10, iters=10, step=0.05, mode="surrogate", bound=None, z_ref=0.78, dt=2e-3,
+                   mu=None, dmass=None, reg=0.1):
+    """Short-horizon refinement of the targets u0 [29, n] a policy chose at
+    state s: `iters` normalised gradient steps on J (of `step` rad in the
+    29-dim target space, per env), each judged by the exact step: an update
+    that does not lower the exact J is rejected and that env's step halved.
+    mode "surrogate": gradients through the surrogate rollout; with `bound`,
+    envs whose surrogate one-step error at s exceeds it fall back to the
+    exact adjoint's gradient.  mode "exact": the exact adjoint only.
+    Returns (u, J_exact per env, fraction of envs on the surrogate's
+    gradient)."""
+    u = u0.clone()
+    n = u.shape[1]
+    J = exact_objective(s, u, H, z_ref, dt, mu, dmass, u0, reg)
+    alpha = torch.full((n,), step, device=u.device)
+    use_sur = torch.ones(n, dtype=torch.bool, device=u.device) if mode == "surrogate" else \
+        torch.zeros(n, dtype=torch.bool, device=u.device)
+    if mode == "surrogate" and bound is not None:
+        err, _, _, _ = one_step_error(sur, {**s, "ctrl": u}, dt, mu, dmass)
+        use_sur &= err <= bound
+    for _ in range(iters):
+        g = torch.zeros_like(u)
+        if bool(use_sur.any()):
+            g = rollout_grad(sur, s, u, H, z_ref, dt, mu, dmass, u0, reg)[1]
+        if not bool(use_sur.all()):
+            g = torch.where(use_sur[None], g, exact_grad(s, u, H, z_ref, dt, u0, reg))
+        d = g / g.norm(dim=0).clamp_min(1e-12)
+        cand = u - alpha[None] * d
+        Jc = exact_objective(s, cand, H, z_ref, dt, mu, dmass, u0, reg)
+        ok = Jc < J
+        u = torch.where(ok[None], cand, u)
+        J = torch.where(ok, Jc, J)
+        alpha = torch.where(ok, alpha, 0.5 * alpha)
+    return u, J, float(use_sur.float().mean().item())

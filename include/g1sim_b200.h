@@ -255,8 +255,7 @@ int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
 int g1b_gemm_status(int* code);
 /* Element-wise kernels of the surrogate: SiLU with transposed copy, its
  * backward with bias-gradient sums, weighted MSE and its gradient, Adam,
- * BF16 weight copies, the feature vector of the state, and the
- * surrogate's state update (qacc -> qvel, qpos). */
+ * BF16 weight copies. */
 int g1b_sur_act(int B, int D, const float* Z, void* H, void* Ht, void* stream);
 int g1b_sur_act_bwd(int B, int D, const float* dH, const float* Z, void* dZ, void* dZt, float* db, void* stream);
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
@@ -264,10 +263,34 @@ int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, v
 int g1b_sur_adam(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
                  int step, void* stream);
 int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* stream);
-int g1b_sur_features(int n, const float* qpos, const float* qvel, const float* ctrl, const float* cf,
-                     const float* mean, const float* istd, void* X, void* Xt, float* F, void* stream);
+/* The surrogate's input features of n envs (159 used of 192: joint angles
+ * and rates, base height, rotation, body-frame velocities, per foot sphere
+ * its penetration depth, contact flag, offset from its anchor and world
+ * velocity, targets, friction, base-mass offset, 1), normalised with
+ * (mean, istd) into BF16 X [n][192] (Xt [192][n] and raw F [n][192]
+ * nullable).  State SoA as in g1b_step; mu, dmass [n] nullable (1, 0). */
+int g1b_sur_features(int n, const float* qpos, const float* qvel, const float* anchor, const float* ctrl,
+                     const float* mu, const float* dmass, const float* mean, const float* istd, void* X, void* Xt,
+                     float* F, void* stream);
+/* Adjoint of the features: dX [n][ld] (FP32) is the adjoint of the
+ * normalised inputs; adds the state adjoint into qpos_b [36][n], qvel_b
+ * [35][n], anchor_b [16][n] (nullable) and the targets' into ctrl_b [29][n]. */
+int g1b_sur_features_vjp(int n, const float* qpos, const float* qvel, const float* anchor, const float* istd,
+                         const float* dX, int ld, float* qpos_b, float* qvel_b, float* anchor_b, float* ctrl_b,
+                         void* stream);
+/* The surrogate's state update in place (qacc = Y * ostd + omean, then the
+ * step's semi-implicit Euler), and its adjoint at the state before the
+ * update: lam_qpos / lam_qvel hold the adjoint of the updated state and are
+ * replaced by the adjoint through the update; dY [n][ldd] gets the adjoint
+ * of the normalised network output. */
 int g1b_sur_integrate(int n, const float* Y, int ldy, const float* omean, const float* ostd, float dt, float* qpos,
                       float* qvel, void* stream);
+int g1b_sur_integrate_vjp(int n, const float* qpos, const float* qvel, const float* Y, int ldy, const float* omean,
+                          const float* ostd, float dt, float* lam_qpos, float* lam_qvel, float* dY, int ldd,
+                          void* stream);
+/* BF16 copy of `total` FP32 values (the seed of the network's input-gradient
+ * products). */
+int g1b_sur_seed(int total, const float* dY, void* dZ, void* stream);
 
 #ifdef __cplusplus
 }
