@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--surrogate-steps", type=int, default=3000, help="training steps of the surrogate (-1: skip)")
-    p.add_argument("--part", default="all", choices=["all", "policy", "adjoint", "gemm", "surrogate"],
+    p.add_argument("--part", default="all", choices=["all", "policy", "adjoint", "gemm", "surrogate", "ppo"],
                    help="one sub-benchmark alone on --nenv envs (rows), one GPU (a small case for a profiler)")
     p.add_argument("--horizon", type=int, default=64, help="adjoint horizon with --part adjoint")
     return p.parse_args()
@@ -372,6 +372,73 @@ def policy_fused_bench(n, rank, device, stream, steps, warmup, world, local, ini
             "status": status, "finite": bool(torch.isfinite(buf.rewards).all().item()), "accuracy": acc}
 
 
+# -------------------------------------------- PPO iteration (config 3)
+PPO_ENVS, PPO_T = 16384, 24
+
+
+def policy_ppo_bench(device, iters=4, n=PPO_ENVS, T=PPO_T):
+    """The policy-fused training workload end to end: per iteration one
+    launch of the fused kernel for T = 24 policy steps of 16,384 envs
+    (decimation 10: observation, critic and actor on the tensor cores,
+    sampling, physics, reward, resets), the observation normaliser update,
+    GAE (gamma 0.99, lambda 0.95) and the PPO update (5 epochs x 4
+    minibatches, Adam, the reference's losses), then the weights repacked for
+    the kernel.  Xavier-initialised network; velocity commands vx, yaw in
+    U[-1, 1], vy in U[-0.5, 0.5].  Also the deviation of the kernel's BF16
+    network from the reference's FP32 ActorCritic.forward on the first
+    rollout's observations."""
+    import torch
+    from g1sim_b200 import g1sim as G
+    from g1sim_b200 import policy as P
+    torch.manual_seed(0)
+    ac = P.ActorCritic().xavier_(torch.Generator().manual_seed(0)).to(device)
+    opt = torch.optim.Adam(ac.parameters(), lr=1e-3)
+    sim = {"qpos": torch.zeros(36, n, device=device), "qvel": torch.zeros(35, n, device=device),
+           "anchor": torch.zeros(16, n, device=device), "ctrl": torch.zeros(29, n, device=device)}
+    for k, d in (("foot_pos", 6), ("foot_vel", 6), ("contact_forces", 8)):
+        sim[k] = torch.zeros(d, n, device=device)
+    G.reset_done(sim["qpos"], sim["qvel"], sim["anchor"], torch.ones(n, dtype=torch.uint8, device=device), seed=42,
+                 noise=0.1, drop=0.02)
+    sim["ctrl"].copy_(sim["qpos"][7:])
+    task = P.TaskState(n, device, seed=0)
+    buf = P.RolloutBuffers(T, n, device, mean=True)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    rows, dev_stats = [], None
+    for it in range(iters):
+        packed = P.pack_policy(ac, device)
+        e0, e1, e2, e3 = ev(), ev(), ev(), ev()
+        e0.record()
+        P.policy_rollout(sim, packed, task, buf, T, decim=DECIM, step0=it * T, seed=it, bootstrap=True)
+        e1.record()
+        if it == 0:
+            with torch.no_grad():
+                obs = buf.obs.reshape(-1, 99)
+                mean32, _ = ac(obs)
+                val32 = ac.critic(ac.normalize_obs(obs)).squeeze(-1)
+                dm = (buf.mean.reshape(-1, 29) - mean32).abs()
+                dv = (buf.values.reshape(-1) - val32).abs()
+                dev_stats = {"samples": int(obs.shape[0]),
+                             "actor_mean_abs_dev": {"median": float(dm.median()), "max": float(dm.max())},
+                             "actor_mean_scale": float(mean32.abs().mean()),
+                             "critic_value_abs_dev": {"median": float(dv.median()), "max": float(dv.max())},
+                             "critic_value_scale": float(val32.abs().mean())}
+        ac.update_obs_norm(buf.obs.reshape(-1, 99))
+        returns, advs = P.gae(buf.rewards, buf.values, buf.dones, buf.last_value, buf.dones[-1])
+        e2.record()
+        kl = P.ppo_update(ac, opt, buf, returns, advs, epochs=5, minibatches=4)
+        e3.record()
+        torch.cuda.synchronize()
+        rows.append({"rollout_ms": e0.elapsed_time(e1), "gae_ms": e1.elapsed_time(e2), "update_ms": e2.elapsed_time(e3),
+                     "mean_reward": float(buf.rewards.mean()), "mean_kl": kl})
+    it_ms = statistics.mean(r["rollout_ms"] + r["gae_ms"] + r["update_ms"] for r in rows[1:] or rows)
+    return {"envs": n, "policy_steps_per_rollout": T, "decimation": DECIM, "iterations": iters,
+            "iteration_ms": it_ms, "env_steps_per_s_with_update": n * T * DECIM / (it_ms * 1e-3),
+            "rollout_ms": statistics.mean(r["rollout_ms"] for r in rows[1:] or rows),
+            "update_ms": statistics.mean(r["update_ms"] for r in rows[1:] or rows),
+            "per_iteration": rows, "bf16_network_vs_fp32_forward": dev_stats,
+            "ppo": "5 epochs x 4 minibatches of 98,304 samples, clip 0.2, Adam lr 1e-3, max grad norm 1"}
+
+
 # ------------------------------------------------------- horizon adjoint
 ADJ_ENVS, ADJ_H, ADJ_C = 4096, 64, 8
 
@@ -602,6 +669,8 @@ def part_only(args, local):
         init = {k: torch.tensor(w[k], dtype=torch.float32, device=device)
                 for k in ("qpos", "qvel", "anchor", "ctrl", "mu", "dmass")}
         r = policy_fused_bench(args.nenv, 0, device, stream, args.steps, args.warmup, 1, local, init)
+    elif args.part == "ppo":
+        r = policy_ppo_bench(device)
     elif args.part == "surrogate":
         r = surrogate_bench(device, args.surrogate_steps, 1)
     elif args.part == "adjoint":
@@ -740,6 +809,7 @@ def ours(args, world, rank, local):
     finite = bool(torch.isfinite(st["qpos"]).all().item())
 
     pol = policy_fused_bench(n, rank, device, stream, args.steps, args.warmup, world, local, init)
+    ppo = policy_ppo_bench(device) if rank == 0 else None
     adj = adjoint_bench(device, stream, args.steps, args.warmup, world) if not args.no_adjoint else None
     sur = surrogate_bench(device, args.surrogate_steps, world) if args.surrogate_steps >= 0 else None
 
@@ -774,6 +844,7 @@ def ours(args, world, rank, local):
             "single_launch": {"value": env_steps / (single_ms * 1e-3), "ms": single_ms},
             "resets_per_timed_step": resets_per_step, "finite": finite, "accuracy": accuracy,
             "policy_fused": pol,
+            "policy_ppo": ppo,
         }
         if adj is not None:
             line["adjoint"] = adj

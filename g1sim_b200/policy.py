@@ -316,8 +316,10 @@ def gae(rewards, values, dones, next_value, next_done, gamma=0.99, lam=0.95):
 
 
 def ppo_update(ac, optimizer, buf, returns, advs, epochs=5, minibatches=4, clip=0.2, max_grad_norm=1.0,
-               generator=None):
-    """PPO epochs x minibatches (reference train.py:330-390).  Returns mean KL."""
+               generator=None, perms=None):
+    """PPO epochs x minibatches (reference train.py:330-390).  Returns mean KL.
+    perms: optional minibatch order, one permutation of the samples per epoch
+    (default: torch.randperm with `generator`)."""
     advs = (advs - advs.mean()) / (advs.std() + 1e-8)
     b_obs = buf.obs.reshape(-1, NOBS)
     b_actions = buf.actions.reshape(-1, NACT)
@@ -328,8 +330,8 @@ def ppo_update(ac, optimizer, buf, returns, advs, epochs=5, minibatches=4, clip=
     n = b_obs.shape[0]
     mb = n // minibatches
     kl_sum, count = 0.0, 0
-    for _ in range(epochs):
-        idx = torch.randperm(n, device=b_obs.device, generator=generator)
+    for ep in range(epochs):
+        idx = perms[ep] if perms is not None else torch.randperm(n, device=b_obs.device, generator=generator)
         for s in range(0, n, mb):
             j = idx[s:s + mb]
             new_logp, values, entropy = ac.evaluate(b_obs[j], b_actions[j])
