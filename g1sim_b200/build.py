@@ -19,8 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libg1cuda.so")
-UNITS = ["g1_step.cu", "g1_step_k32.cu", "g1_step_k64.cu", "g1_step_k96.cu", "g1_step_k128.cu", "g1_policy.cu",
-         "g1_adjoint.cu", "g1_surrogate.cu"]
+UNITS = ["g1_step.cu", "g1_step_k32.cu", "g1_step_k64.cu", "g1_step_k96.cu", "g1_step_k128.cu", "g1_step3_k64.cu",
+         "g1_step3_k128.cu", "g1_policy.cu", "g1_adjoint.cu", "g1_surrogate.cu"]
 SOURCES = [os.path.join(CSRC, u) for u in UNITS]
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(os.path.dirname(HERE), "include", "g1sim_b200.h")]

@@ -451,6 +451,10 @@ constexpr int kSlotXchg = kSlotFoot + 12;
 constexpr int kXUp = kSlotXchg, kXA0 = kSlotXchg + 27, kXBase = kSlotXchg + 33, kXReset = kSlotXchg + 46;
 constexpr int kNumSlotsSingle = kSlotXchg;  // one thread per env
 constexpr int kNumSlots = kSlotXchg + 47;   // two threads per env
+// three threads per env (left leg, right leg, upper body): also the right
+// leg's projection into the pelvis (27)
+constexpr int kXLeg = kNumSlots;
+constexpr int kNumSlots3 = kNumSlots + 27;
 constexpr int kSlotJointState = 2 * kNJ;  // q and qd of every hinge
 G1_CE int hslot(int body, int k) {
   return k < 2 ? k * kNJ + (body - 1) : kSlotJointState + (body - 1) * (kSlotsPerHinge - 2) + (k - 2);
@@ -1052,38 +1056,105 @@ G1_HD void load_base(Scr& scr, EnvState& st) {
 // body's projection into the pelvis, the base acceleration and the base
 // state through the scratch.
 
+// ------------------------------------------ one leg (three-role split)
+// FK of leg c (0 left, 1 right) in extended precision and its contacts;
+// stores the chain end, the foot wrench and (last substep) the foot outputs.
+template <class Scr>
+G1_HD void fk_leg(const EnvState& st, int c, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
+                  bool last_sub) {
+  FKNode n;
+  base_node(st, cfg, n);
+  base_pose_ff(st, n);
+  fk_chain<true>(chain_first(c), chain_last(c), n, scr);
+  const SV wr = foot_contacts(4 * c, n, io, last_sub, cfg, ep.mu);
+  store_sv(scr, kSlotFoot + 6 * c, wr);
+  store_end(scr, c, n);
+  if (last_sub) foot_outputs(n, io, c == 0 ? 0 : 3);
+}
+
+// Backward pass of leg c: its projection into the pelvis frame.
+template <class Scr>
+G1_HD void bwd_leg(int c, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr, AI& outI, SV& outP) {
+  V3 w, v, g;
+  load_end(scr, c, w, v, g);
+  const int last = chain_last(c);
+  const AI IA = body_inertia(body(last));
+  SV pA = bias_force(IA, w, v, g);
+  sv_acc(pA, load_sv(scr, kSlotFoot + 6 * c));
+  bwd_chain(chain_first(c), last, IA, pA, w, v, g, outI, outP, io, ep, cfg, scr);
+}
+
+// The pelvis's own articulated inertia and bias force.
+G1_HD void pelvis_acc(const EnvState& st, const EnvParams& ep, const StepConfig& cfg, AI& acc0, SV& accP0) {
+  FKNode base;
+  base_node(st, cfg, base);
+  acc0 = pelvis_inertia(ep.dmass);
+  accP0 = bias_force(acc0, base.w, base.v, base.g);
+}
+
+// Forward pass of leg c from the base acceleration (st: the base state at
+// the start of the substep).
+template <class Scr>
+G1_HD void fwd_leg(const EnvState& st, int c, const SV& a0, const StepConfig& cfg, Scr& scr) {
+  FKNode base;
+  base_node(st, cfg, base);
+  SV a = a0;
+  V3 w = base.w, v = base.v;
+  fwd_chain(chain_first(c), chain_last(c), a, w, v, cfg.dt, scr);
+}
+
+// Base integration (semi-implicit Euler; the free-joint convention of
+// fwd_lower_and_base).
+G1_HD void integrate_base(EnvState& st, const SV& a0, const StepConfig& cfg) {
+  const float dt = cfg.dt;
+  FKNode base;
+  base_node(st, cfg, base);
+  const V3 al = mv(base.R, add(a0.l, crs(base.w, base.v)));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.vw[k] += dt * al.v[k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
+  const float wx = st.wb[0], wy = st.wb[1], wz = st.wb[2];
+  const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
+  const float angle = wn * dt;
+  if (angle >= 1e-12f) {
+    float sh, ch;
+    sincosf(0.5f * angle, &sh, &ch);
+    const float k = sh / wn;
+    const float dq[4] = {ch, k * wx, k * wy, k * wz};
+    const float* q = st.quat;
+    float r[4];
+    r[0] = q[0] * dq[0] - q[1] * dq[1] - q[2] * dq[2] - q[3] * dq[3];
+    r[1] = q[0] * dq[1] + q[1] * dq[0] + q[2] * dq[3] - q[3] * dq[2];
+    r[2] = q[0] * dq[2] - q[1] * dq[3] + q[2] * dq[0] + q[3] * dq[1];
+    r[3] = q[0] * dq[3] + q[1] * dq[2] - q[2] * dq[1] + q[3] * dq[0];
+    quat_normalized(r, st.quat);
+  }
+}
+
 // FK of the legs in extended precision, contacts; stores chain ends, foot
 // wrenches and (last substep) the foot outputs.
 template <class Scr>
 G1_HD void fk_lower(const EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
                     bool last_sub) {
-  FKNode base;
-  base_node(st, cfg, base);
-  base_pose_ff(st, base);
 #pragma unroll 1
-  for (int c = 0; c < 2; ++c) {
-    FKNode n = base;
-    fk_chain<true>(chain_first(c), chain_last(c), n, scr);
-    const SV wr = foot_contacts(4 * c, n, io, last_sub, cfg, ep.mu);
-    store_sv(scr, kSlotFoot + 6 * c, wr);
-    store_end(scr, c, n);
-    if (last_sub) foot_outputs(n, io, c == 0 ? 0 : 3);
-  }
+  for (int c = 0; c < 2; ++c) fk_leg(st, c, io, ep, cfg, scr, last_sub);
 }
 
-// FK of the waist and the arms; stores chain ends.
+// FK of the waist and the arms (one call site for the three chains);
+// stores chain ends.
 template <class Scr>
 G1_HD void fk_upper(const EnvState& st, const StepConfig& cfg, Scr& scr) {
-  FKNode n;
-  base_node(st, cfg, n);
-  fk_chain<false>(13, 15, n, scr);
-  store_end(scr, 2, n);
-  const FKNode torso = n;
+  FKNode base, torso;
+  base_node(st, cfg, base);
 #pragma unroll 1
-  for (int c = 3; c < 5; ++c) {
-    n = torso;
+  for (int c = 2; c < 5; ++c) {
+    FKNode n = c == 2 ? base : torso;
     fk_chain<false>(chain_first(c), chain_last(c), n, scr);
     store_end(scr, c, n);
+    if (c == 2) torso = n;
   }
 }
 
@@ -1115,23 +1186,12 @@ G1_HD void bwd_upper(const EnvIO& io, const EnvParams& ep, const StepConfig& cfg
 template <class Scr>
 G1_HD void bwd_lower(const EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg, Scr& scr,
                      AI& acc0, SV& accP0) {
-  {
-    FKNode base;
-    base_node(st, cfg, base);
-    acc0 = pelvis_inertia(ep.dmass);
-    accP0 = bias_force(acc0, base.w, base.v, base.g);
-  }
+  pelvis_acc(st, ep, cfg, acc0, accP0);
 #pragma unroll 1
   for (int c = 0; c < 2; ++c) {
-    V3 w, v, g;
-    load_end(scr, c, w, v, g);
-    const int last = chain_last(c);
-    const AI IA = body_inertia(body(last));
-    SV pA = bias_force(IA, w, v, g);
-    sv_acc(pA, load_sv(scr, kSlotFoot + 6 * c));
     AI ci;
     SV cp;
-    bwd_chain(chain_first(c), last, IA, pA, w, v, g, ci, cp, io, ep, cfg, scr);
+    bwd_leg(c, io, ep, cfg, scr, ci, cp);
     ai_add(acc0, ci);
     sv_acc(accP0, cp);
   }
@@ -1142,39 +1202,9 @@ G1_HD void bwd_lower(const EnvState& st, const EnvIO& io, const EnvParams& ep, c
 // body angular, reference src/g1_core.h:203-206,215-220).
 template <class Scr>
 G1_HD void fwd_lower_and_base(EnvState& st, const SV& a0, const StepConfig& cfg, Scr& scr) {
-  const float dt = cfg.dt;
-  FKNode base;
-  base_node(st, cfg, base);
 #pragma unroll 1
-  for (int c = 0; c < 2; ++c) {
-    SV a = a0;
-    V3 w = base.w, v = base.v;
-    fwd_chain(chain_first(c), chain_last(c), a, w, v, dt, scr);
-  }
-  const V3 al = mv(base.R, add(a0.l, crs(base.w, base.v)));
-#pragma unroll
-  for (int k = 0; k < 3; ++k) st.vw[k] += dt * al.v[k];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) st.wb[k] += dt * a0.a.v[k];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) st.pos[k] += dt * st.vw[k];
-  // q <- q (x) exp(w dt / 2), renormalised (reference src/spatial.h:73-79)
-  const float wx = st.wb[0], wy = st.wb[1], wz = st.wb[2];
-  const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
-  const float angle = wn * dt;
-  if (angle >= 1e-12f) {
-    float sh, ch;
-    sincosf(0.5f * angle, &sh, &ch);
-    const float k = sh / wn;
-    const float dq[4] = {ch, k * wx, k * wy, k * wz};
-    const float* q = st.quat;
-    float r[4];
-    r[0] = q[0] * dq[0] - q[1] * dq[1] - q[2] * dq[2] - q[3] * dq[3];
-    r[1] = q[0] * dq[1] + q[1] * dq[0] + q[2] * dq[3] - q[3] * dq[2];
-    r[2] = q[0] * dq[2] - q[1] * dq[3] + q[2] * dq[0] + q[3] * dq[1];
-    r[3] = q[0] * dq[3] + q[1] * dq[2] - q[2] * dq[1] + q[3] * dq[0];
-    quat_normalized(r, st.quat);
-  }
+  for (int c = 0; c < 2; ++c) fwd_leg(st, c, a0, cfg, scr);
+  integrate_base(st, a0, cfg);
 }
 
 // Forward pass of the waist and the arms (the base state is not touched).
@@ -1195,6 +1225,93 @@ G1_HD void fwd_upper(const EnvState& st, const SV& a0, const StepConfig& cfg, Sc
     v = v15;
     fwd_chain(chain_first(c), chain_last(c), a, w, v, dt, scr);
   }
+}
+
+// ------------------------------------- role-driven phases (split step)
+// The backward and forward passes of either role of the two-thread split
+// step through one call site each, so that one compiled copy of the chain
+// routines serves both roles' warps (instruction fetch is the step's largest
+// stall).  The arithmetic is that of bwd_lower / bwd_upper and
+// fwd_lower_and_base / fwd_upper, in the same order.
+// role 0: the legs into the pelvis accumulator (pelvis inertia and bias
+// included); role 1: the arms into the torso, then the waist into the
+// pelvis frame.
+template <class Scr>
+G1_HD void bwd_role(int role, const EnvState& st, const EnvIO& io, const EnvParams& ep, const StepConfig& cfg,
+                    Scr& scr, AI& outI, SV& outP) {
+  AI acc;
+  SV accP;
+  V3 w15, v15, g15;
+  if (role == 0) {
+    pelvis_acc(st, ep, cfg, acc, accP);
+  } else {
+    load_end(scr, 2, w15, v15, g15);
+    acc = body_inertia(body(15));
+    accP = bias_force(acc, w15, v15, g15);
+  }
+  const int nch = role == 0 ? 2 : 3;
+#pragma unroll 1
+  for (int k = 0; k < nch; ++k) {
+    const int c = role == 0 ? k : (k < 2 ? 3 + k : 2);
+    AI IA;
+    SV pA;
+    V3 w, v, g;
+    if (c == 2) {
+      IA = acc;
+      pA = accP;
+      w = w15;
+      v = v15;
+      g = g15;
+    } else {
+      load_end(scr, c, w, v, g);
+      IA = body_inertia(body(chain_last(c)));
+      pA = bias_force(IA, w, v, g);
+      if (c < 2) sv_acc(pA, load_sv(scr, kSlotFoot + 6 * c));
+    }
+    AI ci;
+    SV cp;
+    bwd_chain(chain_first(c), chain_last(c), IA, pA, w, v, g, ci, cp, io, ep, cfg, scr);
+    if (c == 2) {
+      outI = ci;
+      outP = cp;
+    } else {
+      ai_add(acc, ci);
+      sv_acc(accP, cp);
+    }
+  }
+  if (role == 0) {
+    outI = acc;
+    outP = accP;
+  }
+}
+
+// role 0: the legs, then the base integration of st; role 1: the waist,
+// then the arms from the torso (st untouched).
+template <class Scr>
+G1_HD void fwd_role(int role, EnvState& st, const SV& a0, const StepConfig& cfg, Scr& scr) {
+  FKNode base;
+  base_node(st, cfg, base);
+  SV a15;
+  V3 w15, v15;
+  const int nch = role == 0 ? 2 : 3;
+#pragma unroll 1
+  for (int k = 0; k < nch; ++k) {
+    const int c = role == 0 ? k : 2 + k;
+    SV a = a0;
+    V3 w = base.w, v = base.v;
+    if (c > 2) {
+      a = a15;
+      w = w15;
+      v = v15;
+    }
+    fwd_chain(chain_first(c), chain_last(c), a, w, v, cfg.dt, scr);
+    if (c == 2) {
+      a15 = a;
+      w15 = w;
+      v15 = v;
+    }
+  }
+  if (role == 0) integrate_base(st, a0, cfg);
 }
 
 // One substep on one thread: FK -> contacts -> PD + ABA -> integrate

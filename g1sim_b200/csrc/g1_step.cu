@@ -96,6 +96,10 @@ LaunchShape current_shape() {
 
 int dispatch(const LaunchShape& L, bool rollout, const StateArgs& a, float* ctrl, int* rc, int nouter,
              int ninner, const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s) {
+  if (L.mapping == 2) {
+    if (L.block == 64) return run_split3<64>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+    return run_split3<128>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
+  }
   if (L.mapping == 1) {
     switch (L.block) {
       case 32: return run_split<32>(rollout, a, ctrl, rc, nouter, ninner, cfg, rp, s, L.bps);
@@ -191,8 +195,10 @@ void g1_cuda_reset_done(int nenv, float* qpos, float* qvel, float* anchor, const
 }
 
 int g1b_set_launch(int mapping, int block, int blocks_per_sm) {
-  if (mapping != 0 && mapping != 1) return fail("mapping must be 0 (thread per env) or 1 (two threads per env)");
+  if (mapping < 0 || mapping > 2)
+    return fail("mapping must be 0 (thread per env), 1 (two threads per env) or 2 (three threads per env)");
   if (block != 32 && block != 64 && block != 96 && block != 128) return fail("block must be 32, 64, 96 or 128");
+  if (mapping == 2 && block != 64 && block != 128) return fail("mapping 2 takes block 64 or 128");
   if (blocks_per_sm < 0) return fail("blocks_per_sm must be >= 0");
   std::lock_guard<std::mutex> lk(g_mu);
   g_mapping = mapping;
@@ -230,9 +236,10 @@ int g1b_autotune(int nenv, int nsub, void* stream, float* best_ms) {
   LaunchShape best{1, 128, 0};
   float best_t = 1e30f;
   int rc = 0;
-  for (int mapping = 0; mapping < 2 && rc == 0; ++mapping) {
+  for (int mapping = 0; mapping < 3 && rc == 0; ++mapping) {
     for (int bi = 0; bi < 4 && rc == 0; ++bi) {
       const LaunchShape L{mapping, blocks[bi], 0};
+      if (mapping == 2 && blocks[bi] != 64 && blocks[bi] != 128) continue;
       init_stand_kernel<<<(nenv + 127) / 128, 128, 0, st>>>(nenv, qpos, qvel, anchor, ctrl);
       rc = dispatch(L, false, a, ctrl, nullptr, 1, 1, cfg, rp, st);  // warm-up
       if (rc) break;

@@ -14,6 +14,12 @@ int run_single(bool rollout, const StateArgs& a, float* ctrl, int* rc, int noute
 template <int ENVS>
 int run_split(bool rollout, const StateArgs& a, float* ctrl, int* rc, int nouter, int ninner,
               const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s, int bps);
+// mapping 2: three threads per env (ENVS envs, 3 ENVS threads per CTA)
+template <int ENVS>
+int run_split3(bool rollout, const StateArgs& a, float* ctrl, int* rc, int nouter, int ninner,
+               const StepConfig& cfg, const RolloutParams& rp, cudaStream_t s, int bps);
+template <> int run_split3<64>(bool, const StateArgs&, float*, int*, int, int, const StepConfig&, const RolloutParams&, cudaStream_t, int);
+template <> int run_split3<128>(bool, const StateArgs&, float*, int*, int, int, const StepConfig&, const RolloutParams&, cudaStream_t, int);
 template <> int run_single<32>(bool, const StateArgs&, float*, int*, int, int, const StepConfig&, const RolloutParams&, cudaStream_t, int);
 template <> int run_single<64>(bool, const StateArgs&, float*, int*, int, int, const StepConfig&, const RolloutParams&, cudaStream_t, int);
 template <> int run_single<96>(bool, const StateArgs&, float*, int*, int, int, const StepConfig&, const RolloutParams&, cudaStream_t, int);

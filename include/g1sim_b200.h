@@ -84,10 +84,12 @@ int g1b_rollout(int nenv, int npolicy, int decim, const g1b_config* cfg,
 /* Launch shape of the step kernels.  mapping 0: one thread per env, block =
  * envs (= threads) per block; mapping 1 (default): two threads per env, the
  * lower body (pelvis, legs, contacts, base) and the upper body (waist, arms)
- * on separate warps, block = envs per block (2 * block threads).  block is
- * 32, 64, 96 or 128; blocks_per_sm caps the persistent grid (0 = all that
- * fit).  g1b_autotune times the candidates on the current device for a
- * workload of nenv envs and keeps the fastest; g1b_get_launch reports it. */
+ * on separate warps, block = envs per block (2 * block threads); mapping 2:
+ * three threads per env (left leg with the pelvis and base, right leg, upper
+ * body), block 64 or 128 (3 * block threads).  block is 32, 64, 96 or 128;
+ * blocks_per_sm caps the persistent grid (0 = all that fit).  g1b_autotune
+ * times the candidates on the current device for a workload of nenv envs
+ * and keeps the fastest; g1b_get_launch reports it. */
 int g1b_set_launch(int mapping, int block, int blocks_per_sm);
 int g1b_get_launch(int* mapping, int* block, int* blocks_per_sm);
 int g1b_autotune(int nenv, int nsub, void* stream, float* best_ms);
