@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--surrogate-steps", type=int, default=3000, help="training steps of the surrogate (-1: skip)")
-    p.add_argument("--part", default="all", choices=["all", "policy", "adjoint", "gemm", "surrogate", "ppo"],
+    p.add_argument("--part", default="all", choices=["all", "plain", "policy", "adjoint", "gemm", "surrogate", "ppo"],
                    help="one sub-benchmark alone on --nenv envs (rows), one GPU (a small case for a profiler)")
     p.add_argument("--horizon", type=int, default=64, help="adjoint horizon with --part adjoint")
     return p.parse_args()
@@ -594,6 +594,32 @@ def surrogate_bench(device, train_steps, world):
             "gemm_status": S.gemm_status()}
 
 
+def plain_bench(device, n, steps, warmup):
+    """The plain step alone: one policy step (10 substeps, target redraw,
+    reset check) of n randomised envs per launch, `warmup` + `steps`
+    launches, CUDA-event timed (a small case for a profiler)."""
+    import torch
+    from g1sim_b200 import _lib, workloads
+    from g1sim_b200 import g1sim as G
+    w = workloads.randomized(nenv=n, seed=0)
+    st = {k: torch.tensor(w[k], dtype=torch.float32, device=device)
+          for k in ("qpos", "qvel", "anchor", "ctrl", "mu", "dmass")}
+    run = lambda k: G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 1, DECIM, config=_cfg(), seed=0,  # noqa
+                              step0=k, mu=st["mu"], dmass=st["dmass"])
+    for k in range(warmup):
+        run(k)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(steps):
+        run(warmup + k)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(steps, 1)
+    mapping, block, _ = _lib.get_launch()
+    return {"ms_per_launch": ms, "env_steps_per_s": n * DECIM / (ms * 1e-3),
+            "tflops": FLOPS_PER_ENV_STEP * n * DECIM / (ms * 1e-3) / 1e12, "mapping": mapping, "block": block}
+
+
 def _cfg():
     from g1sim_b200 import _lib
     return _lib.default_config(dt=DT)
@@ -663,7 +689,9 @@ def part_only(args, local):
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     stream = torch.cuda.Stream(device)
-    if args.part == "policy":
+    if args.part == "plain":
+        r = plain_bench(device, args.nenv, args.steps, args.warmup)
+    elif args.part == "policy":
         from g1sim_b200 import workloads
         w = workloads.randomized(nenv=args.nenv, seed=0)
         init = {k: torch.tensor(w[k], dtype=torch.float32, device=device)
