@@ -658,28 +658,57 @@ def refinement_bench(sur, device, n=4096, H=50, iters=10):
 
 
 def gemm_bench(device, rows, steps, warmup):
-    """One surrogate hidden-layer product alone: C[rows x 512] = A[rows x 512]
-    . W[512 x 512]^T + b (g1b_gemm_bf16), timed over `steps` calls."""
+    """The surrogate's layer products alone, rows x 512 x 512, each timed over
+    `steps` calls with CUDA events: the plain product C = A W^T + b (FP32 C,
+    g1b_gemm_bf16), the fused hidden layer of training (FP32 Z, BF16 H and
+    H^T) and of inference (BF16 H only), the fused backward through SiLU (BF16
+    dZ and dZ^T, bias-gradient sums) and the weight gradient (K = rows split
+    over tiles, atomic FP32 sums).  hbm_gbs: algorithmic bytes (operands read
+    once, outputs written once) per call over its time."""
     import torch
     from g1sim_b200 import surrogate as S
     g = torch.Generator(device=device).manual_seed(0)
-    A_ = torch.randn(rows, 512, device=device, generator=g).to(torch.bfloat16)
-    W = torch.randn(512, 512, device=device, generator=g).to(torch.bfloat16)
+    bf = torch.bfloat16
+    A_ = torch.randn(rows, 512, device=device, generator=g).to(bf)
+    W = (torch.randn(512, 512, device=device, generator=g) / 512 ** 0.5).to(bf)
     b = torch.randn(512, device=device, generator=g)
     C_ = torch.empty(rows, 512, device=device)
-    for _ in range(max(1, warmup)):
-        S.gemm(A_, W, C_, bias=b)
-    torch.cuda.synchronize()
+    Z = torch.randn(rows, 512, device=device, generator=g)
+    H = torch.empty(rows, 512, dtype=bf, device=device)
+    Ht = torch.empty(512, rows, dtype=bf, device=device)
+    At = torch.randn(512, rows, device=device, generator=g).to(bf)
+    db = torch.zeros(512, device=device)
+    Cw = torch.empty(512, 512, device=device)
+    splits = max(1, min(64, rows // 2048))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(max(1, steps)):
-        S.gemm(A_, W, C_, bias=b)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / max(1, steps)
-    return {"shape": [rows, 512, 512], "us_per_call": ms * 1e3,
-            "tflops": 2.0 * rows * 512 * 512 / (ms * 1e-3) / 1e12, "status": S.gemm_status()}
+
+    def timed(fn):
+        for _ in range(max(1, warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(max(1, steps)):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / max(1, steps)
+
+    flops = 2.0 * rows * 512 * 512
+    el = rows * 512
+    cases = [("store", lambda: S.gemm(A_, W, C_, bias=b), el * (2 + 4)),
+             ("silu_forward_training", lambda: S.linear_silu(A_, W, b, H, Z=C_, Ht=Ht), el * (2 + 4 + 2 + 2)),
+             ("silu_forward_inference", lambda: S.linear_silu(A_, W, b, H), el * (2 + 2)),
+             ("silu_backward", lambda: S.linear_silu_bwd(A_, W, Z, H, dHt=Ht, db=db), el * (2 + 4 + 2 + 2)),
+             ("weight_gradient", lambda: S.gemm(At, Ht, Cw, splits=splits), el * (2 + 2))]
+    modes = {}
+    for name, fn, nbytes in cases:
+        ms = timed(fn)
+        modes[name] = {"us_per_call": ms * 1e3, "tflops": flops / (ms * 1e-3) / 1e12,
+                       "hbm_gbs": nbytes / (ms * 1e-3) / 1e9, "algorithmic_bytes": nbytes}
+    return {"shape": [rows, 512, 512], "us_per_call": modes["store"]["us_per_call"],
+            "tflops": modes["store"]["tflops"], "modes": modes, "weight_gradient_splits": splits,
+            "status": S.gemm_status()}
 
 
 def part_only(args, local):

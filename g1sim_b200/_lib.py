@@ -93,8 +93,10 @@ def lib():
     L.g1b_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,
                                 _vp]
     L.g1b_gemm_status.argtypes = [C.POINTER(C.c_int)]
-    L.g1b_sur_act.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
-    L.g1b_sur_act_bwd.argtypes = [C.c_int, C.c_int] + [_vp] * 6
+    L.g1b_sur_linear_silu.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int,
+                                                       _vp, C.c_int, _vp]
+    L.g1b_sur_linear_silu_bwd.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,
+                                                           _vp, C.c_int, _vp, _vp]
     L.g1b_sur_loss.argtypes = [C.c_int, C.c_int] + [_vp] * 8
     L.g1b_sur_adam.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _vp]
     L.g1b_sur_cast.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]

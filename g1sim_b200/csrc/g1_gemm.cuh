@@ -1,173 +1,516 @@
-// g1_gemm.cuh -- BF16 tcgen05 GEMM for the dynamics-surrogate training
-// (included by g1_kernels.cu inside namespace g1b, after g1_mlp.cuh).
+// g1_gemm.cuh -- persistent BF16 tcgen05 GEMM with TMA operand loads and
+// TMA-stored fused epilogues, for the dynamics surrogate (included by
+// g1_surrogate.cu inside namespace g1b, after g1_mlp.cuh).
 //
-//   C[M x N] (= or +=) A[M x K] . B[N x K]^T (+ bias[N])
-// A and B are BF16, row-major with K contiguous (leading dimensions lda,
-// ldb in elements); C is FP32 row-major (ldc).  One CTA (128 threads) owns
-// a 128 MT x Nt tile of C (MT = 1 or 2 row tiles, Nt = min(N, 256), an MMA's N) and a K range of its
-// split: 64-wide K chunks are copied global -> shared with 16-byte cp.async
-// into the UMMA 128-byte-swizzle K-major layout (kGemmStages-deep ring), thread 0 issues
-// tcgen05.mma (M 128, K 16) into a tensor-memory accumulator, and the four
-// warps read their 32 lanes back for the epilogue.  With several K splits
-// the partial tiles are added into C with atomics (C zeroed by the caller).
+//   C[M x N] = A[M x K] . B[N x K]^T, A and B BF16 row-major with K
+//   contiguous, FP32 accumulation in tensor memory, and one of four
+//   epilogues (GemmMode):
+//     kGemmStore    C (FP32) = acc (+ bias)
+//     kGemmAtomic   C (FP32) += acc (+ bias on the first K split): K split
+//                   over tiles, C cleared by the caller
+//     kGemmSilu     z = acc + bias; Z (FP32, nullable) = z,
+//                   H (BF16) = silu(z), Ht (BF16, transposed [N][M], nullable)
+//     kGemmSiluBwd  g = acc * silu'(Zin); H (BF16) = g, Ht = g transposed
+//                   (nullable), db[N] += column sums of g (nullable)
+//
+// One CTA per SM (320 threads) walks the tiles blockIdx.x, + gridDim.x, ...
+// of 128 rows x Nt columns (Nt = min(N, 256)) and K split, row tiles
+// outermost so that the column tiles of one row block run close together
+// and read its A rows from L2.  Warp roles:
+//   warp 0   (one lane) TMA producer: for every 64-wide K chunk of a tile,
+//            waits until the MMAs have released the stage, then copies the
+//            A chunk (128 x 64) and the B chunk (Nt x 64) with
+//            cp.async.bulk.tensor (tensor maps over this GPU's memory, no
+//            multicast) into a kGemmStages-deep ring; the copies complete on
+//            the stage's `full` mbarrier (transaction bytes);
+//   warp 1   (one lane) MMA issuer: per chunk waits on `full`, issues four
+//            tcgen05.mma (M 128, N Nt, K 16) into one of two tensor-memory
+//            accumulators and commits them to the stage's `empty` barrier;
+//            after a tile's last chunk commits to the accumulator's `full`
+//            barrier, and before a tile waits until the epilogue has
+//            drained that accumulator (its `empty` barrier, one arrival per
+//            epilogue warp);
+//   warps 2-9 epilogue, two per TMEM lane quarter (warp w may access lanes
+//            32 (w % 4) .. + 31, i.e. 32 rows of the tile), one taking the
+//            even and one the odd 32-column groups: tcgen05.ld, the mode's
+//            arithmetic, then the 32 x 32 results go to the warp's staging
+//            buffer in shared memory in the layout of the output's tensor
+//            map and one lane stores them with cp.async.bulk.tensor (whole
+//            lines to global memory instead of one row per lane).  Two
+//            warps per SM sub-partition hide each other's latencies, and the
+//            MMAs of the next tile run on the other accumulator meanwhile.
+//            The backward mode's pre-activation Z comes in the same way, one
+//            step ahead (TMA load into the staging buffer, one mbarrier per
+//            warp).  The bias of the warp's columns is staged once per tile.
+// Operand tiles land in the UMMA K-major 128-byte-swizzle layout (each row's
+// 64 values one 128-byte line, eight lines a 1024-byte atom, 16-byte piece j
+// of row r at piece j ^ (r % 8)), the tensor map's SWIZZLE_128B.  Staging
+// layouts: FP32 32 x 32 boxes with SWIZZLE_128B (row r, piece j at
+// j ^ (r % 8)), BF16 32 x 32 boxes (64-byte rows) with SWIZZLE_64B (piece j
+// at j ^ ((r / 2) % 4)), the transposed BF16 boxes unswizzled: each is
+// conflict-free for the lane-per-row writes.  A column group narrower than
+// 32 (N % 32 == 16) is written with plain stores instead, so that no box
+// reaches into a neighbouring tile.
+//
+// Every wait is bounded (tc::kWaitNs).  A wait that gives up raises the
+// CTA's abort flag and the kernel's error flag; every role then stops
+// issuing work, the producer waits (bounded) until the copies it issued have
+// landed, the MMA lane until the MMAs it issued are complete, the epilogue
+// until its loads and stores have finished, and the tensor memory is
+// released.
 //
 // Constraints (checked by the host launcher): M % 128 == 0, N % 16 == 0,
-// N % Nt == 0, K % (64 * splits) == 0, lda / ldb multiples of 8.
+// N % Nt == 0, K % (64 splits) == 0, lda / ldb / ldh / ldt multiples of 8,
+// ldc / ldz of 4, 16-byte aligned operands.
 
-constexpr int kGemmKC = 64;  // K columns per chunk
+constexpr int kGemmKC = 64;  // K columns per chunk (one 128-byte swizzle line)
 constexpr int kGemmMaxN = 256;
+constexpr int kGemmStages = 3;
+constexpr int kGemmEpiWarps = 8;  // two per TMEM lane quarter
+constexpr int kGemmThreads = 64 + 32 * kGemmEpiWarps;
 constexpr uint32_t kGemmABytes = 128 * kGemmKC * 2;        // 16 KB
 constexpr uint32_t kGemmBBytes = kGemmMaxN * kGemmKC * 2;  // 32 KB
-// MT row tiles of 128 per CTA share each B chunk (MT = 2 halves the weight
-// traffic per row, the bound of this kernel); the ring holds 192 KB.
-template <int MT>
-__host__ __device__ constexpr uint32_t gemm_stage_bytes() { return MT * kGemmABytes + kGemmBBytes; }
-template <int MT>
-__host__ __device__ constexpr int gemm_stages() { return MT == 2 ? 3 : 4; }
-template <int MT>
-__host__ __device__ constexpr size_t gemm_smem() {
-  return gemm_stages<MT>() * (size_t)gemm_stage_bytes<MT>() + 1024;  // + alignment slack
+constexpr uint32_t kGemmStageBytes = kGemmABytes + kGemmBBytes;
+constexpr uint32_t kGemmAccCols = 256;  // one accumulator; two of them fill the 512 TMEM columns
+// Per epilogue warp one staging slot of: FP32 box 4 KB (output C / Z, or
+// the Z input), BF16 box 2 KB (H), transposed BF16 box 2 KB (Ht); and the
+// bias of its columns of the tile (128 floats).
+constexpr uint32_t kEpiF = 0, kEpiH = 4096, kEpiT = 6144, kEpiWarpBytes = 8192, kEpiBiasBytes = 512;
+constexpr size_t kGemmSmem = kGemmStages * (size_t)kGemmStageBytes +
+                             kGemmEpiWarps * (size_t)(kEpiWarpBytes + kEpiBiasBytes) + 1024;
+
+enum GemmMode : int { kGemmStore = 0, kGemmAtomic = 1, kGemmSilu = 2, kGemmSiluBwd = 3 };
+
+struct GemmArgs {
+  int ntm, ntn, splits, nk;  // row tiles, column tiles, K splits, chunks per split
+  int Nt;                    // columns per tile
+  float* C;                  // store / atomic: C; silu: Z (nullable)
+  int ldc;
+  const float* bias;  // [N], nullable (store, atomic, silu)
+  __nv_bfloat16* H;   // silu: silu(z); silu_bwd: g
+  int ldh;
+  __nv_bfloat16* Ht;  // transposed copy [N][ldt], nullable
+  int ldt;
+  const float* Z;  // silu_bwd: the pre-activation
+  int ldz;
+  float* db;  // silu_bwd: column sums, nullable
+  int* err;
+};
+
+// The output tensor maps (a map the mode does not use holds a valid dummy).
+struct GemmOutMaps {
+  CUtensorMap f;  // FP32 [M][N] box 32 x 32, SWIZZLE_128B: C, Z (silu), Zin (silu_bwd)
+  CUtensorMap h;  // BF16 [M][N] box 32 x 32, SWIZZLE_64B: H
+  CUtensorMap t;  // BF16 [N][M] box 32 x 32, no swizzle: Ht
+};
+
+// SiLU and its derivative.  Both results are rounded to BF16 (8 significant
+// bits) before they are used, so the hardware exponential and division
+// (relative errors ~2^-21) sit far inside that rounding; for z < -87 the
+// denominator overflows to infinity and both return 0.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Copy K chunk [k0, k0 + 64) of rows [r0, r0 + rows) of a row-major BF16
-// matrix into shared memory at dst (1024-byte aligned) in the UMMA K-major
-// 128-byte-swizzle layout: each row's 64 values are one 128-byte line, eight
-// lines form a 1024-byte atom, and the 16-byte piece j of row r sits at piece
-// position j ^ (r % 8) of its line (bank-conflict-free for the tensor core).
-__device__ __forceinline__ void gemm_load_tile(uint32_t dst, const __nv_bfloat16* X, int ld, int r0, int rows,
-                                               int k0) {
-  const int pieces = rows * (kGemmKC / 8);
-  for (int p = threadIdx.x; p < pieces; p += 128) {
-    const int r = p >> 3, j = p & 7;
-    const __nv_bfloat16* src = X + (size_t)(r0 + r) * ld + k0 + j * 8;
-    const uint32_t off = (uint32_t)(r >> 3) * 1024u + (uint32_t)(r & 7) * 128u + (uint32_t)((j ^ (r & 7)) * 16);
-    cp_async16(dst + off, src);
-  }
-}
-// Shared-memory descriptor of such a tile, K step kk (16 values = 32 bytes
-// along the line): swizzle mode 128B (2), stride between 8-row atoms 1024 B.
+// Shared-memory descriptor of a swizzled K-major tile at K step kk (16
+// values = 32 bytes along the line): layout SWIZZLE_128B (2), stride between
+// 8-row atoms 1024 B, version 1.
 __device__ __forceinline__ uint64_t gemm_desc_sw128(uint32_t tile, int kk) {
   const uint32_t a = tile + (uint32_t)kk * 32u;
   return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) |
          (2ull << 61);
 }
 
-template <bool kAtomic, int MT>
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
-                                                        const __nv_bfloat16* __restrict__ B, int ldb, float* C,
-                                                        int ldc, const float* __restrict__ bias, int Nt, int Ks,
-                                                        int* err) {
-  constexpr int kGemmStages = gemm_stages<MT>();
-  constexpr uint32_t kGemmStage = gemm_stage_bytes<MT>();
-  constexpr uint32_t kBOff = MT * kGemmABytes;
-  constexpr uint32_t kCols = 256 * MT;
+// 2-D tiled TMA load of the box at (x, y) (x the inner coordinate, a
+// multiple of 16 bytes) into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+// 2-D tiled TMA store of a staged box to (x, y) >= 0, in the bulk group of
+// the issuing thread.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// No committed group of this thread still reading shared memory.
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Every committed group of this thread complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void gemm_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Bounded wait that also gives up as soon as another role raised the abort flag.
+__device__ __forceinline__ bool gemm_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  if (tc::mbar_try(bar, parity)) return true;
+  const uint64_t t0 = tc::globaltimer();
+  while (!tc::mbar_try(bar, parity)) {
+    if (*abort_flag) return false;
+    if (tc::globaltimer() - t0 > tc::kWaitNs) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+struct GemmTile {
+  int m, n, sp;
+};
+__device__ __forceinline__ GemmTile gemm_tile(const GemmArgs& g, int t) {
+  const int per = g.ntm * g.ntn;
+  const int sp = t / per, r = t - sp * per;
+  return {r / g.ntn, r % g.ntn, sp};
+}
+
+// ------------------------------------------------------------ epilogue
+// Staging writes of one lane's row r (0..31) of a 32 x 32 box.
+// FP32 box, SWIZZLE_128B: 128-byte rows, 16-byte piece j at j ^ (r % 8).
+__device__ __forceinline__ void stage_f32(uint8_t* box, int r, const float (&v)[32]) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    *reinterpret_cast<float4*>(box + r * 128 + ((j ^ (r & 7)) << 4)) =
+        make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+}
+__device__ __forceinline__ void unstage_f32(const uint8_t* box, int r, float (&v)[32]) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float4 q = *reinterpret_cast<const float4*>(box + r * 128 + ((j ^ (r & 7)) << 4));
+    v[4 * j] = q.x;
+    v[4 * j + 1] = q.y;
+    v[4 * j + 2] = q.z;
+    v[4 * j + 3] = q.w;
+  }
+}
+// BF16 box, SWIZZLE_64B: 64-byte rows, 16-byte piece j (8 values) at j ^ ((r / 2) % 4).
+__device__ __forceinline__ void stage_bf16(uint8_t* box, int r, const float (&v)[32]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    uint4 w;
+    w.x = tc::pack_bf16x2(v[8 * j], v[8 * j + 1]);
+    w.y = tc::pack_bf16x2(v[8 * j + 2], v[8 * j + 3]);
+    w.z = tc::pack_bf16x2(v[8 * j + 4], v[8 * j + 5]);
+    w.w = tc::pack_bf16x2(v[8 * j + 6], v[8 * j + 7]);
+    *reinterpret_cast<uint4*>(box + r * 64 + ((j ^ ((r >> 1) & 3)) << 4)) = w;
+  }
+}
+// Transposed BF16 box, no swizzle: element (column i, row r) at i * 64 + 2 r.
+__device__ __forceinline__ void stage_bf16_t(uint8_t* box, int r, const float (&v)[32]) {
+  __nv_bfloat16* b = reinterpret_cast<__nv_bfloat16*>(box);
+#pragma unroll
+  for (int i = 0; i < 32; ++i) b[i * 32 + r] = __float2bfloat16_rn(v[i]);
+}
+
+// Plain stores of a narrow group (nb < 32 columns) or of the atomic mode:
+// FP32 row to C (store, atomic add), BF16 row to H and its transpose to Ht.
+template <bool kAtomic>
+__device__ __forceinline__ void direct_f32(float* crow, const float (&v)[32], int nb) {
+  if (nb == 32) {
+#pragma unroll
+    for (int i = 0; i < 32; i += 4) {
+      const float4 q = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      if (kAtomic)
+        atomicAdd(reinterpret_cast<float4*>(crow + i), q);
+      else
+        *reinterpret_cast<float4*>(crow + i) = q;
+    }
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    if (i >= nb) continue;
+    if (kAtomic)
+      atomicAdd(crow + i, v[i]);
+    else
+      crow[i] = v[i];
+  }
+}
+__device__ __forceinline__ void direct_bf16(const GemmArgs& g, const float (&v)[32], int row, int col, int nb) {
+  __nv_bfloat16* h = g.H + (size_t)row * g.ldh + col;
+#pragma unroll
+  for (int i = 0; i < 32; ++i)
+    if (i < nb) h[i] = __float2bfloat16_rn(v[i]);
+  if (g.Ht) {
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+      if (i < nb) g.Ht[(size_t)(col + i) * g.ldt + row] = __float2bfloat16_rn(v[i]);
+  }
+}
+
+// Column sums over the warp's 32 rows (lane = row) into db[col .. col + nb):
+// recursive halving across the lanes, five shuffle levels (16 + 8 + 4 + 2 +
+// 1 exchanges), after which lane l holds the sum of column l.
+__device__ __forceinline__ void column_sums(float* db, const float (&v)[32], int col, int nb) {
+  const int lane = threadIdx.x & 31;
+  float w[16];
+  {
+    const bool hi = lane & 16;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const float send = hi ? v[i] : v[i + 16];
+      w[i] = (hi ? v[i + 16] : v[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+  }
+#pragma unroll
+  for (int off = 8; off >= 1; off >>= 1) {
+    const bool hi = lane & off;
+#pragma unroll
+    for (int i = 0; i < off; ++i) {
+      const float send = hi ? w[i] : w[i + off];
+      w[i] = (hi ? w[i + off] : w[i]) + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  if (lane < nb) atomicAdd(db + col + lane, w[0]);
+}
+
+// The epilogue role (warps 2 .. 2 + kGemmEpiWarps - 1).  Warp w owns TMEM
+// lane quarter w % 4 (rows 32 (w % 4) .. + 31 of the tile) and, of the tile's
+// 32-column groups, the even ones (w < 6) or the odd ones (w >= 6).  mf / mh
+// / mt: the output maps (kernel parameters, so their generic addresses stay
+// valid for TMA).
+template <int kMode>
+__device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorMap* mf, const CUtensorMap* mh,
+                                              const CUtensorMap* mt, uint32_t tmem, uint8_t* ep0, uint32_t ebase0,
+                                              uint64_t* zbar, uint64_t* accf, uint64_t* acce, int ntiles,
+                                              volatile int* abort_v) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = warp & 3;   // TMEM lane quarter = the warp's 32 rows of the tile
+  const int ew = warp - 2;  // staging area and mbarrier of this warp
+  const int par = ew >> 2;  // the warp's column groups: par, par + 2, ...
+  uint8_t* const ep = ep0 + (size_t)ew * kEpiWarpBytes;
+  const uint32_t es = ebase0 + (uint32_t)ew * kEpiWarpBytes;
+  float* const sbias = reinterpret_cast<float*>(ep0 + (size_t)kGemmEpiWarps * kEpiWarpBytes + ew * kEpiBiasBytes);
+  const uint32_t zb = tc::smem_u32(&zbar[ew]);
+  const bool st_f = kMode == kGemmStore || (kMode == kGemmSilu && g.C != nullptr);
+  const bool st_h = kMode == kGemmSilu || kMode == kGemmSiluBwd;
+  const bool st_t = st_h && g.Ht != nullptr;
+  const bool has_bias = g.bias != nullptr && kMode != kGemmSiluBwd;
+  const int ngroups = (g.Nt + 31) / 32;
+  const int spw = (ngroups - par + 1) / 2;  // this warp's groups per tile
+  const int my_tiles = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nsteps = my_tiles * spw;
+  bool ok = true;
+  int zi = 0, zw = 0;  // backward: Z boxes issued, waited for
+  // backward: TMA load of the Z box of step k (this warp's rows and group)
+  auto z_issue = [&](int k) {
+    if (lane == 0) {
+      const GemmTile tl = gemm_tile(g, (int)blockIdx.x + (k / spw) * (int)gridDim.x);
+      tc::fence_async_smem();
+      tc::mbar_expect_tx(zb, 4096);
+      tma_load_2d(es + kEpiF, mf, tl.n * g.Nt + (2 * (k % spw) + par) * 32, tl.m * 128 + q * 32, zb);
+    }
+    ++zi;
+  };
+  if (kMode == kGemmSiluBwd && nsteps > 0) z_issue(0);
+  int k = 0, j = 0;
+  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++j) {
+    const GemmTile tl = gemm_tile(g, t);
+    const int b = j & 1;
+    if (has_bias && (kMode != kGemmAtomic || tl.sp == 0)) {  // this warp's bias values of the tile
+      __syncwarp();
+      for (int s = 0; s < spw; ++s) {
+        const int c = (2 * s + par) * 32 + lane;
+        sbias[s * 32 + lane] = c < g.Nt ? __ldg(g.bias + tl.n * g.Nt + c) : 0.0f;  // exactly N floats
+      }
+      __syncwarp();
+    }
+    // every wait of the epilogue is warp-uniform (the warp's tcgen05.ld are .sync.aligned)
+    if (!__all_sync(0xffffffffu, gemm_wait(tc::smem_u32(&accf[b]), ((uint32_t)j >> 1) & 1, abort_v))) {
+      ok = false;
+      break;
+    }
+    tc::tc_fence_after();
+    const int row0 = tl.m * 128 + q * 32, row = row0 + lane;
+    const uint32_t taddr = tmem + (uint32_t)b * kGemmAccCols + ((uint32_t)(q * 32) << 16);
+    for (int s = 0; s < spw; ++s, ++k) {
+      const int c = (2 * s + par) * 32;
+      const int nb = g.Nt - c < 32 ? g.Nt - c : 32;
+      const int col = tl.n * g.Nt + c;
+      float v[32];
+      tc::tmem_ld32(taddr + (uint32_t)c, v);
+      if (kMode == kGemmSiluBwd) {
+        if (!__all_sync(0xffffffffu, gemm_wait(zb, (uint32_t)k & 1, abort_v))) {
+          ok = false;
+          break;
+        }
+        ++zw;
+        float z[32];
+        unstage_f32(ep + kEpiF, lane, z);
+        __syncwarp();  // every lane has read the box: the next one may land in its place
+        if (k + 1 < nsteps) z_issue(k + 1);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
+        if (g.db) column_sums(g.db, v, col, nb);
+      } else if (has_bias && (kMode != kGemmAtomic || tl.sp == 0)) {
+        const float4* bq = reinterpret_cast<const float4*>(sbias + s * 32);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float4 bb = bq[i];  // same address in every lane: a broadcast
+          v[4 * i] += bb.x;
+          v[4 * i + 1] += bb.y;
+          v[4 * i + 2] += bb.z;
+          v[4 * i + 3] += bb.w;
+        }
+      }
+      if (kMode == kGemmAtomic) {
+        direct_f32<true>(g.C + (size_t)row * g.ldc + col, v, nb);
+        continue;
+      }
+      float hv[32];  // the BF16 output's values
+#pragma unroll
+      for (int i = 0; i < 32; ++i) hv[i] = kMode == kGemmSilu ? silu(v[i]) : v[i];
+      if (nb < 32) {  // narrow group: plain stores
+        if (st_f) direct_f32<false>(g.C + (size_t)row * g.ldc + col, v, nb);
+        if (st_h) direct_bf16(g, hv, row, col, nb);
+        continue;
+      }
+      if (lane == 0) bulk_wait_read0();  // the previous step's stores have read the slot
+      __syncwarp();
+      if (st_f) stage_f32(ep + kEpiF, lane, v);
+      if (st_h) stage_bf16(ep + kEpiH, lane, hv);
+      if (st_t) stage_bf16_t(ep + kEpiT, lane, hv);
+      tc::fence_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        if (st_f) tma_store_2d(mf, col, row0, es + kEpiF);
+        if (st_h) tma_store_2d(mh, col, row0, es + kEpiH);
+        if (st_t) tma_store_2d(mt, row0, col, es + kEpiT);
+        bulk_commit();
+      }
+    }
+    if (!ok) break;
+    tc::tc_fence_before();
+    __syncwarp();
+    if (lane == 0) gemm_arrive(tc::smem_u32(&acce[b]));
+  }
+  // the Z boxes issued and not waited for have landed, the stores have completed
+  for (; zw < zi; ++zw)
+    if (!tc::mbar_wait(zb, (uint32_t)zw & 1)) ok = false;
+  if (lane == 0) bulk_wait_all();
+  __syncwarp();
+  return ok;
+}
+
+// ---------------------------------------------------------------- kernel
+template <int kMode>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ GemmOutMaps om, GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t gsm[];
-  __shared__ uint64_t bars[kGemmStages + 1];  // mma done per stage, accumulator
+  __shared__ uint64_t full[kGemmStages], empty[kGemmStages], accf[2], acce[2], drain, zbar[kGemmEpiWarps];
   __shared__ uint32_t tslot;
-  const int m0 = blockIdx.x * 128 * MT, n0 = blockIdx.y * Nt, kbeg = blockIdx.z * Ks;
-  const int nchunks = Ks / kGemmKC;
-  const uint32_t sbase = (tc::smem_u32(gsm) + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
-  const uint32_t bacc = tc::smem_u32(&bars[kGemmStages]);
+  __shared__ int abort_flag;
+  volatile int* abort_v = &abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t base0 = tc::smem_u32(gsm);
+  const uint32_t sbase = (base0 + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
+  const uint32_t ebase0 = sbase + (uint32_t)kGemmStages * kGemmStageBytes;  // epilogue staging
+  const int ntiles = g.ntm * g.ntn * g.splits;
+  const uint32_t btx = (uint32_t)g.Nt * kGemmKC * 2;  // B bytes per chunk
   if (threadIdx.x == 0) {
-    for (int i = 0; i <= kGemmStages; ++i) tc::mbar_init(tc::smem_u32(&bars[i]), 1);
+    for (int s = 0; s < kGemmStages; ++s) {
+      tc::mbar_init(tc::smem_u32(&full[s]), 1);
+      tc::mbar_init(tc::smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(tc::smem_u32(&accf[b]), 1);
+      tc::mbar_init(tc::smem_u32(&acce[b]), kGemmEpiWarps);
+    }
+    for (int w = 0; w < kGemmEpiWarps; ++w) tc::mbar_init(tc::smem_u32(&zbar[w]), 1);
+    tc::mbar_init(tc::smem_u32(&drain), 1);
+    abort_flag = 0;
     tc::mbar_fence_init();
   }
-  if (threadIdx.x < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tslot)),
-                 "r"(kCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), 2 * kGemmAccCols);
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tslot;
-  const uint32_t idesc = tc::idesc_bf16(128, Nt);
   bool ok = true;
 
-  // prologue: chunks 0 .. kGemmStages - 2 (one commit group each, empty groups past the end)
-  for (int i = 0; i < kGemmStages - 1; ++i) {
-    if (i < nchunks) {
-      const uint32_t st = sbase + (uint32_t)i * kGemmStage;
-      gemm_load_tile(st, A, lda, m0, 128 * MT, kbeg + i * kGemmKC);
-      gemm_load_tile(st + kBOff, B, ldb, n0, Nt, kbeg + i * kGemmKC);
-    }
-    cp_async_commit();
-  }
-  for (int c = 0; c < nchunks; ++c) {
-    const int s = c % kGemmStages;
-    cp_async_wait<kGemmStages - 2>();  // this thread's copies of chunk c have landed
-    tc::fence_async_smem();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      tc::tc_fence_after();
-      const uint32_t st = sbase + (uint32_t)s * kGemmStage;
-#pragma unroll
-      for (int j = 0; j < kGemmKC / 16; ++j)
-#pragma unroll
-        for (int t = 0; t < MT; ++t)
-          tc::mma_bf16(tmem + (uint32_t)(t * 256), gemm_desc_sw128(st + (uint32_t)t * kGemmABytes, j),
-                       gemm_desc_sw128(st + kBOff, j), idesc, (c > 0 || j > 0) ? 1u : 0u);
-      tc::mma_commit(tc::smem_u32(&bars[s]));
-      if (c + 1 == nchunks) tc::mma_commit(bacc);
-    }
-    // refill the stage read by chunk c - 1 with chunk c + kGemmStages - 1
-    const int nx = c + kGemmStages - 1;
-    if (nx < nchunks) {
-      const int sp = nx % kGemmStages;
-      if (c >= 1 && !tc::mbar_wait(tc::smem_u32(&bars[sp]), ((c - 1) / kGemmStages) & 1)) ok = false;
-      const uint32_t st = sbase + (uint32_t)sp * kGemmStage;
-      gemm_load_tile(st, A, lda, m0, 128 * MT, kbeg + nx * kGemmKC);
-      gemm_load_tile(st + kBOff, B, ldb, n0, Nt, kbeg + nx * kGemmKC);
-    }
-    cp_async_commit();
-  }
-  if (!tc::mbar_wait(bacc, 0)) ok = false;
-  tc::tc_fence_after();
-  // epilogue: warp w holds rows 32 w .. 32 w + 31 of each 128-row subtile
-  for (int t = 0; t < MT; ++t) {
-    const int row = m0 + t * 128 + (int)threadIdx.x;
-    const uint32_t lane_base = tmem + (uint32_t)(t * 256) + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
-    float* crow = C + (size_t)row * ldc + n0;
-    for (int c = 0; c < Nt; c += 32) {
-      float v[32];
-      tc::tmem_ld32(lane_base + (uint32_t)c, v);
-      if (bias && blockIdx.z == 0) {
-        const int nb = Nt - c < 32 ? Nt - c : 32;  // the bias holds exactly N floats
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-          if (i < nb) v[i] += __ldg(bias + n0 + c + i);
-      }
-      if (c + 32 > Nt) {  // Nt = 16 or 48 ...: partial last group
-        for (int i = 0; i < Nt - c; ++i) {
-          if (kAtomic)
-            atomicAdd(crow + c + i, v[i]);
-          else
-            crow[c + i] = v[i];
+  if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+      uint32_t it = 0;  // chunks issued by this CTA
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const GemmTile tl = gemm_tile(g, t);
+        for (int c = 0; c < g.nk; ++c) {
+          const int s = (int)(it % kGemmStages);
+          const uint32_t r = it / kGemmStages;
+          if (r > 0 && !gemm_wait(tc::smem_u32(&empty[s]), (r - 1) & 1, abort_v)) {
+            ok = false;
+            break;
+          }
+          const uint32_t st = sbase + (uint32_t)s * kGemmStageBytes;
+          const uint32_t bar = tc::smem_u32(&full[s]);
+          const int kx = (tl.sp * g.nk + c) * kGemmKC;
+          tc::mbar_expect_tx(bar, kGemmABytes + btx);
+          tma_load_2d(st, &tmA, kx, tl.m * 128, bar);
+          tma_load_2d(st + kGemmABytes, &tmB, kx, tl.n * g.Nt, bar);
+          ++it;
         }
-      } else if (kAtomic) {
-#pragma unroll
-        for (int i = 0; i < 32; ++i) atomicAdd(crow + c + i, v[i]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 32; i += 4)
-          *reinterpret_cast<float4*>(crow + c + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      }
+      // every copy issued has landed before the CTA may exit
+      for (int s = 0; s < kGemmStages; ++s) {
+        const uint32_t n_s = it > (uint32_t)s ? (it - (uint32_t)s - 1) / kGemmStages + 1 : 0;
+        if (n_s > 0 && !tc::mbar_wait(tc::smem_u32(&full[s]), (n_s - 1) & 1)) ok = false;
       }
     }
+  } else if (warp == 1) {
+    if (lane == 0) {  // ---- MMA issuer
+      const uint32_t idesc = tc::idesc_bf16(128, g.Nt);
+      uint32_t it = 0;
+      int j = 0;  // tiles of this CTA
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++j) {
+        const int b = j & 1;
+        const uint32_t u = (uint32_t)j >> 1;
+        if (u > 0 && !gemm_wait(tc::smem_u32(&acce[b]), (u - 1) & 1, abort_v)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)b * kGemmAccCols;
+        for (int c = 0; c < g.nk; ++c, ++it) {
+          const int s = (int)(it % kGemmStages);
+          const uint32_t r = it / kGemmStages;
+          if (!gemm_wait(tc::smem_u32(&full[s]), r & 1, abort_v)) {
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t st = sbase + (uint32_t)s * kGemmStageBytes;
+#pragma unroll
+          for (int kk = 0; kk < kGemmKC / 16; ++kk)
+            tc::mma_bf16(d, gemm_desc_sw128(st, kk), gemm_desc_sw128(st + kGemmABytes, kk), idesc,
+                         (c > 0 || kk > 0) ? 1u : 0u);
+          tc::mma_commit(tc::smem_u32(&empty[s]));
+        }
+        if (!ok) break;
+        tc::mma_commit(tc::smem_u32(&accf[b]));
+      }
+      // every MMA issued is complete before the tensor memory is released
+      tc::mma_commit(tc::smem_u32(&drain));
+      if (!tc::mbar_wait(tc::smem_u32(&drain), 0)) ok = false;
+    }
+  } else {
+    ok = gemm_epilogue<kMode>(g, &om.f, &om.h, &om.t, tmem, gsm + (ebase0 - base0), ebase0, zbar, accf, acce, ntiles,
+                              abort_v);
   }
-  if (!ok) atomicExch(err, 1);
+  if (!ok) {
+    *abort_v = 1;
+    atomicExch(g.err, 1);
+  }
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
-  if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+  if (warp == 0) tc::tmem_dealloc(tmem, 2 * kGemmAccCols);
 }

@@ -19,6 +19,11 @@ inline int fail(const char* msg) {
   snprintf(g_err, sizeof(g_err), "%s", msg);
   return -1;
 }
+template <class... Args>
+inline int failf(const char* fmt, Args... args) {
+  snprintf(g_err, sizeof(g_err), fmt, args...);
+  return -1;
+}
 inline int cuda_fail(cudaError_t e, const char* where) {
   snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
   return -2;

@@ -1,11 +1,16 @@
 // g1_surrogate.cu -- the learned dynamics surrogate's kernels and their
 // C-ABI: the tcgen05 BF16 GEMM (g1_gemm.cuh) and the element-wise forward,
 // backward, loss, Adam, feature and integration kernels (g1_surrogate.cuh).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #include "g1_host.h"
 #include "g1_mlp.cuh"
@@ -19,45 +24,137 @@ __device__ int g_gemm_error = 0;
 
 using namespace g1b;
 
+// Tensor map of a row-major [rows x cols] matrix (leading dimension ld
+// elements of esize bytes) read or written in boxes of box_cols x box_rows.
+static int gemm_map(CUtensorMap* map, const void* base, CUtensorMapDataType type, int esize, int rows, int cols,
+                    int ld, int box_cols, int box_rows, CUtensorMapSwizzle swz) {
+  static std::atomic<void*> fn{nullptr};
+  void* f = fn.load();
+  if (!f) {
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f)
+      return fail("gemm: cuTensorMapEncodeTiled is not available");
+    fn.store(f);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * (cuuint64_t)esize};
+  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f)(
+      map, type, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : failf("gemm: tensor map encoding failed (CUresult %d)", (int)r);
+}
+static int map_bf16_operand(CUtensorMap* m, const void* p, int rows, int cols, int ld, int box_rows) {
+  return gemm_map(m, p, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, rows, cols, ld, kGemmKC, box_rows,
+                  CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+// Shape checks, tensor maps and the persistent launch of gemm_kernel<kMode>
+// (one CTA per SM, at most one per tile).
+template <int kMode>
+static int gemm_run(const char* what, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                    int splits, GemmArgs g, cudaStream_t st, bool clear_c = false) {
+  if (M <= 0 || N <= 0 || K <= 0 || !A || !B) return failf("%s: invalid arguments", what);
+  if (splits < 1) splits = 1;
+  const int Nt = N <= kGemmMaxN ? N : kGemmMaxN;
+  if (M % 128 || N % 16 || N % Nt || K % (kGemmKC * splits))
+    return failf("%s: needs M %% 128 == 0, N %% 16 == 0 (and N %% 256 == 0 above 256), K %% (64 splits) == 0",
+                 what);
+  if (lda % 8 || ldb % 8 || lda < K || ldb < K || (((uintptr_t)A | (uintptr_t)B) & 15))
+    return failf("%s: lda, ldb multiples of 8 and >= K, 16-byte aligned operands", what);
+  if (g.Ht && (g.ldt % 8 || ((uintptr_t)g.Ht & 15)))
+    return failf("%s: the transposed output needs ldt %% 8 == 0 and 16-byte alignment", what);
+  CUtensorMap ma, mb;
+  GemmOutMaps om;
+  memset(&om, 0, sizeof(om));
+  if (map_bf16_operand(&ma, A, M, K, lda, 128) || map_bf16_operand(&mb, B, N, K, ldb, Nt)) return -1;
+  const float* fsrc = kMode == kGemmSiluBwd ? g.Z : g.C;  // FP32 box: C, Z out, or Z in
+  const int fld = kMode == kGemmSiluBwd ? g.ldz : g.ldc;
+  if (fsrc && kMode != kGemmAtomic &&
+      gemm_map(&om.f, fsrc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, M, N, fld, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B))
+    return -1;
+  if (g.H && gemm_map(&om.h, g.H, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, M, N, g.ldh, 32, 32,
+                      CU_TENSOR_MAP_SWIZZLE_64B))
+    return -1;
+  if (g.Ht && gemm_map(&om.t, g.Ht, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, N, M, g.ldt, 32, 32,
+                       CU_TENSOR_MAP_SWIZZLE_NONE))
+    return -1;
+  cudaError_t e = cudaGetSymbolAddress((void**)&g.err, g_gemm_error);
+  if (e != cudaSuccess) return cuda_fail(e, "gemm: error flag");
+  if (clear_c && (e = cudaMemset2DAsync(g.C, (size_t)g.ldc * 4, 0, (size_t)N * 4, M, st)) != cudaSuccess)
+    return cuda_fail(e, "gemm: clear C");
+  g.ntm = M / 128;
+  g.ntn = N / Nt;
+  g.splits = splits;
+  g.nk = K / (kGemmKC * splits);
+  g.Nt = Nt;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ntiles = g.ntm * g.ntn * splits;
+  const int grid = ntiles < sms ? ntiles : sms;
+  if ((e = prepare<20, kMode>(gemm_kernel<kMode>, kGemmSmem)) != cudaSuccess)
+    return cuda_fail(e, "gemm: attributes");
+  gemm_kernel<kMode><<<grid, kGemmThreads, kGemmSmem, st>>>(ma, mb, om, g);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_fail(e, "gemm_kernel");
+}
+
 extern "C" {
 
 // ------------------------------------------------- surrogate kernels
 int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                   const float* bias, int splits, void* stream) {
-  if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) return fail("gemm_bf16: invalid arguments");
-  if (splits < 1) splits = 1;
-  const int Nt = N <= kGemmMaxN ? N : kGemmMaxN;
-  if (M % 128 || N % 16 || N % Nt || K % (kGemmKC * splits))
-    return fail("gemm_bf16: needs M % 128 == 0, N % 16 == 0 (and N % 256 == 0 above 256), K % (64 splits) == 0");
-  if (lda % 8 || ldb % 8 || ldc % 4 || (((uintptr_t)A | (uintptr_t)B) & 15) || (((uintptr_t)C) & 15))
-    return fail("gemm_bf16: lda, ldb multiples of 8, ldc of 4, 16-byte aligned pointers");
+  if (!C || ldc < N || ldc % 4 || ((uintptr_t)C & 15))
+    return fail("gemm_bf16: C needs ldc >= N, ldc % 4 == 0, 16-byte alignment");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int MT = M % 256 == 0 ? 2 : 1;  // two row tiles per CTA share each weight chunk
-  const dim3 grid(M / (128 * MT), N / Nt, splits);
-  int* err = nullptr;
-  cudaError_t e = cudaGetSymbolAddress((void**)&err, g_gemm_error);
-  if (e != cudaSuccess) return cuda_fail(e, "gemm_bf16: error flag");
-  const __nv_bfloat16* a = static_cast<const __nv_bfloat16*>(A);
-  const __nv_bfloat16* b = static_cast<const __nv_bfloat16*>(B);
-  if (splits > 1) {
-    e = cudaMemset2DAsync(C, (size_t)ldc * 4, 0, (size_t)N * 4, M, st);
-    if (e != cudaSuccess) return cuda_fail(e, "gemm_bf16: clear C");
-  }
-#define G1_GEMM_LAUNCH(AT, M_T, KEY)                                                              \
-  do {                                                                                           \
-    if ((e = prepare<20, KEY>(gemm_bf16_kernel<AT, M_T>, gemm_smem<M_T>())) != cudaSuccess)      \
-      return cuda_fail(e, "gemm_bf16: attributes");                                              \
-    gemm_bf16_kernel<AT, M_T><<<grid, 128, gemm_smem<M_T>(), st>>>(a, lda, b, ldb, C, ldc, bias, Nt, \
-                                                                  K / splits, err);              \
-  } while (0)
-  if (splits > 1) {
-    if (MT == 2) G1_GEMM_LAUNCH(true, 2, 3); else G1_GEMM_LAUNCH(true, 1, 1);
-  } else {
-    if (MT == 2) G1_GEMM_LAUNCH(false, 2, 2); else G1_GEMM_LAUNCH(false, 1, 0);
-  }
-#undef G1_GEMM_LAUNCH
-  e = cudaGetLastError();
-  return e == cudaSuccess ? 0 : cuda_fail(e, "gemm_bf16_kernel");
+  GemmArgs g{};
+  g.C = C;
+  g.ldc = ldc;
+  g.bias = bias;
+  if (splits > 1) return gemm_run<kGemmAtomic>("gemm_bf16", M, N, K, A, lda, B, ldb, splits, g, st, true);
+  return gemm_run<kGemmStore>("gemm_bf16", M, N, K, A, lda, B, ldb, 1, g, st);
+}
+
+int g1b_sur_linear_silu(int M, int N, int K, const void* A, int lda, const void* W, int ldw, const float* bias,
+                        float* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream) {
+  if (!H || ldh < N || ldh % 8 || ((uintptr_t)H & 15))
+    return fail("sur_linear_silu: H needs ldh >= N, ldh % 8 == 0, 16-byte alignment");
+  if (Z && (ldz < N || ldz % 4 || ((uintptr_t)Z & 15)))
+    return fail("sur_linear_silu: Z needs ldz >= N, ldz % 4 == 0, 16-byte alignment");
+  if (Ht && ldt < M) return fail("sur_linear_silu: Ht needs ldt >= M");
+  GemmArgs g{};
+  g.C = Z;
+  g.ldc = ldz;
+  g.bias = bias;
+  g.H = static_cast<__nv_bfloat16*>(H);
+  g.ldh = ldh;
+  g.Ht = static_cast<__nv_bfloat16*>(Ht);
+  g.ldt = ldt;
+  return gemm_run<kGemmSilu>("sur_linear_silu", M, N, K, A, lda, W, ldw, 1, g, static_cast<cudaStream_t>(stream));
+}
+
+int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const void* W, int ldw, const float* Z,
+                            int ldz, void* dH, int ldh, void* dHt, int ldt, float* db, void* stream) {
+  if (!Z || ldz < N || ldz % 4 || ((uintptr_t)Z & 15))
+    return fail("sur_linear_silu_bwd: Z needs ldz >= N, ldz % 4 == 0, 16-byte alignment");
+  if (!dH || ldh < N || ldh % 8 || ((uintptr_t)dH & 15))
+    return fail("sur_linear_silu_bwd: dH needs ldh >= N, ldh % 8 == 0, 16-byte alignment");
+  if (dHt && ldt < M) return fail("sur_linear_silu_bwd: dHt needs ldt >= M");
+  if (dH == dZ) return fail("sur_linear_silu_bwd: dH must not alias dZ");
+  GemmArgs g{};
+  g.H = static_cast<__nv_bfloat16*>(dH);
+  g.ldh = ldh;
+  g.Ht = static_cast<__nv_bfloat16*>(dHt);
+  g.ldt = ldt;
+  g.Z = Z;
+  g.ldz = ldz;
+  g.db = db;
+  return gemm_run<kGemmSiluBwd>("sur_linear_silu_bwd", M, N, K, dZ, ldd, W, ldw, 1, g,
+                                static_cast<cudaStream_t>(stream));
 }
 
 int g1b_gemm_status(int* code) {
@@ -74,22 +171,6 @@ int g1b_gemm_status(int* code) {
 static int grid_1d(size_t n, int block) {
   const size_t g = (n + block - 1) / block;
   return (int)(g < 148 * 16 ? g : 148 * 16);
-}
-
-int g1b_sur_act(int B, int D, const float* Z, void* H, void* Ht, void* stream) {
-  if (B <= 0 || D <= 0 || !Z || !H) return fail("sur_act: invalid arguments");
-  const dim3 grid((D + 31) / 32, (B + 31) / 32), block(32, 8);
-  sur_act_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
-      B, D, Z, static_cast<__nv_bfloat16*>(H), static_cast<__nv_bfloat16*>(Ht));
-  return launched("sur_act_kernel");
-}
-
-int g1b_sur_act_bwd(int B, int D, const float* dH, const float* Z, void* dZ, void* dZt, float* db, void* stream) {
-  if (B <= 0 || D <= 0 || !dH || !Z || !dZ || !dZt || !db) return fail("sur_act_bwd: invalid arguments");
-  const dim3 grid((D + 31) / 32, (B + 31) / 32), block(32, 8);
-  sur_act_bwd_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
-      B, D, dH, Z, static_cast<__nv_bfloat16*>(dZ), static_cast<__nv_bfloat16*>(dZt), db);
-  return launched("sur_act_bwd_kernel");
 }
 
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,

@@ -7,7 +7,7 @@
 // acceleration of the step (the state delta is dt * qacc for qvel, and qpos
 // follows by the step's own semi-implicit Euler).  The feature and update
 // kernels also have their vector-Jacobian products, so that a loss can be
-// differentiated through a surrogate rollout.  Its matrix products run on gemm_bf16_kernel
+// differentiated through a surrogate rollout.  Its matrix products run on gemm_kernel
 // (tcgen05); the element-wise parts of the forward and backward passes, the
 // loss, Adam and the feature extraction are the kernels below.
 
@@ -15,68 +15,12 @@ using sur::kSurFeat;
 using sur::kSurIn;
 constexpr int kSurOut = 64;  // padded outputs (35 used: qacc)
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
-__device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + expf(-z));
-  return s * (1.0f + z * (1.0f - s));
-}
+// silu and silu_grad: g1_gemm.cuh (its fused epilogues use them too).
 
-// The element-wise kernels below work on 32 x 32 tiles (block 32 x 8): rows
+// The loss kernel below works on 32 x 32 tiles (block 32 x 8): rows
 // r0..r0+31 of the batch and columns c0..c0+31, reading and writing the
 // row-major arrays along columns and the transposed copies along rows
 // through a shared-memory tile, so both sides are coalesced.
-
-// H = SiLU(Z) (BF16, [B][D]) and its transpose Ht ([D][B], nullable).
-__global__ void sur_act_kernel(int B, int D, const float* __restrict__ Z, __nv_bfloat16* H, __nv_bfloat16* Ht) {
-  __shared__ __nv_bfloat16 t[32][34];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  for (int k = threadIdx.y; k < 32; k += 8) {
-    const int r = r0 + k, c = c0 + threadIdx.x;
-    if (r < B && c < D) {
-      const size_t i = (size_t)r * D + c;
-      const __nv_bfloat16 h = __float2bfloat16_rn(silu(Z[i]));
-      H[i] = h;
-      t[k][threadIdx.x] = h;
-    }
-  }
-  if (!Ht) return;
-  __syncthreads();
-  for (int k = threadIdx.y; k < 32; k += 8) {
-    const int c = c0 + k, r = r0 + threadIdx.x;
-    if (r < B && c < D) Ht[(size_t)c * B + r] = t[threadIdx.x][k];
-  }
-}
-
-// dZ = dH * SiLU'(Z): BF16 [B][D] and transposed [D][B]; db[c] += column sums.
-__global__ void sur_act_bwd_kernel(int B, int D, const float* __restrict__ dH, const float* __restrict__ Z,
-                                   __nv_bfloat16* dZ, __nv_bfloat16* dZt, float* db) {
-  __shared__ __nv_bfloat16 t[32][34];
-  __shared__ float red[8][33];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  float acc = 0.0f;
-  for (int k = threadIdx.y; k < 32; k += 8) {
-    const int r = r0 + k, c = c0 + threadIdx.x;
-    if (r < B && c < D) {
-      const size_t i = (size_t)r * D + c;
-      const float g = dH[i] * silu_grad(Z[i]);
-      acc += g;
-      const __nv_bfloat16 gb = __float2bfloat16_rn(g);
-      dZ[i] = gb;
-      t[k][threadIdx.x] = gb;
-    }
-  }
-  red[threadIdx.y][threadIdx.x] = acc;
-  __syncthreads();
-  for (int k = threadIdx.y; k < 32; k += 8) {
-    const int c = c0 + k, r = r0 + threadIdx.x;
-    if (r < B && c < D) dZt[(size_t)c * B + r] = t[threadIdx.x][k];
-  }
-  if (threadIdx.y == 0 && c0 + threadIdx.x < D) {
-    float s = 0.0f;
-    for (int k = 0; k < 8; ++k) s += red[k][threadIdx.x];
-    atomicAdd(db + c0 + threadIdx.x, s);
-  }
-}
 
 // Weighted MSE over the output columns: loss += sum_r sum_c w[c] (Y - T)^2 / B;
 // dY = 2 w[c] (Y - T) / B as BF16 [B][D] and transposed [D][B]; db += sums.

@@ -60,6 +60,34 @@ def gemm(A, B, C_, bias=None, splits=1):
                                         _p(bias), splits, _st(A.device)), "g1b_gemm_bf16")
 
 
+def linear_silu(A, W, bias, H, Z=None, Ht=None):
+    """One hidden layer, fused: z = A @ W^T + bias; H = bf16(silu(z)) [M, N];
+    Z = z (FP32 [M, N], optional); Ht = H^T ([N, M] BF16, optional)."""
+    M_, K = A.shape
+    N = W.shape[0]
+    assert W.shape[1] == K and H.shape == (M_, N) and A.dtype == W.dtype == torch.bfloat16
+    assert Z is None or Z.shape == (M_, N)
+    assert Ht is None or (Ht.shape[0] == N and Ht.shape[1] >= M_)
+    _lib.check(_lib.lib().g1b_sur_linear_silu(M_, N, K, _p(A), A.stride(0), _p(W), W.stride(0), _p(bias), _p(Z),
+                                              Z.stride(0) if Z is not None else 0, _p(H), H.stride(0), _p(Ht),
+                                              Ht.stride(0) if Ht is not None else 0, _st(A.device)),
+               "g1b_sur_linear_silu")
+
+
+def linear_silu_bwd(dZ, Wt, Z, dH, dHt=None, db=None):
+    """Backward through a layer and the previous activation, fused:
+    g = (dZ @ Wt^T) * silu'(Z); dH = bf16(g) [M, N]; dHt = dH^T (optional);
+    db += column sums of g (optional).  dH must not share memory with dZ."""
+    M_, K = dZ.shape
+    N = Wt.shape[0]
+    assert Wt.shape[1] == K and dH.shape == (M_, N) and Z.shape[0] == M_ and Z.shape[1] >= N
+    assert dHt is None or (dHt.shape[0] == N and dHt.shape[1] >= M_)
+    _lib.check(_lib.lib().g1b_sur_linear_silu_bwd(M_, N, K, _p(dZ), dZ.stride(0), _p(Wt), Wt.stride(0), _p(Z),
+                                                  Z.stride(0), _p(dH), dH.stride(0), _p(dHt),
+                                                  dHt.stride(0) if dHt is not None else 0, _p(db), _st(dZ.device)),
+               "g1b_sur_linear_silu_bwd")
+
+
 def gemm_status():
     c = C.c_int()
     _lib.check(_lib.lib().g1b_gemm_status(C.byref(c)), "g1b_gemm_status")
@@ -112,11 +140,10 @@ class Surrogate:
                 Z=[None] + [torch.empty(B, DIMS[i], device=d) for i in range(1, 6)],
                 H=[None] + [torch.empty(B, DIMS[i], dtype=bf, device=d) for i in range(1, 5)],
                 Ht=[None] + [torch.empty(DIMS[i], B, dtype=bf, device=d) for i in range(1, 5)],
-                dH=torch.empty(B, 512, device=d),
                 dX=torch.empty(B, NIN, device=d),
                 dY=torch.zeros(B, 64, device=d),
-                db=torch.zeros(512, device=d),
                 dZ=torch.empty(B, 512, dtype=bf, device=d),
+                dZ2=torch.empty(B, 512, dtype=bf, device=d),
                 dZt=torch.zeros(512, B, dtype=bf, device=d),
                 loss=torch.zeros(1, device=d))
         return self._ws[B]
@@ -135,12 +162,11 @@ class Surrogate:
         w = self._work(B)
         L = _lib.lib()
         h = X
-        for i in range(5):
-            gemm(h, self.Wb[i], w["Z"][i + 1], bias=self.b[i])
-            if i < 4:
-                _lib.check(L.g1b_sur_act(B, DIMS[i + 1], _p(w["Z"][i + 1]), _p(w["H"][i + 1]),
-                                         _p(w["Ht"][i + 1]) if keep else None, _st(self.device)), "sur_act")
-                h = w["H"][i + 1]
+        for i in range(4):  # hidden layers: GEMM, bias and SiLU in one kernel
+            linear_silu(h, self.Wb[i], self.b[i], w["H"][i + 1], Z=w["Z"][i + 1] if keep else None,
+                        Ht=w["Ht"][i + 1] if keep else None)
+            h = w["H"][i + 1]
+        gemm(h, self.Wb[4], w["Z"][5], bias=self.b[4])
         return w["Z"][5]
 
     def backward(self, X, Xt, T, want_dx=False, weights=None):
@@ -161,18 +187,18 @@ class Surrogate:
         # dY = d loss / d Y as BF16 [B][64] (start of dZ) and [64][B] (rows of dZt)
         _lib.check(L.g1b_sur_loss(B, 64, _p(w["Z"][5]), _p(T), _p(wv), _p(dZ), _p(dZt), _p(self.gb[4]),
                                   _p(w["loss"]), st), "sur_loss")
+        bufs = [w["dZ"], w["dZ2"]]  # the layer's dZ and the previous layer's, alternating
         for i in range(4, -1, -1):
             Din, Dout = DIMS[i], DIMS[i + 1]
-            dz = dZ.view(-1)[:B * Dout].view(B, Dout)
+            dz = bufs[i & 1].view(-1)[:B * Dout].view(B, Dout)
             rows = max(Dout, 128)
             hin_t = w["Ht"][i] if i > 0 else Xt
             # dW_i = dZ_i^T . H_{i-1} (split over the batch, atomically summed)
             gemm(dZt[:rows], hin_t, self.gW[i][:rows], splits=max(1, min(64, B // 2048)))
             if i > 0:
-                dh = w["dH"].view(-1)[:B * Din].view(B, Din)
-                gemm(dz, self.Wt[i], dh)  # dH_{i-1} = dZ_i . W_i
-                _lib.check(L.g1b_sur_act_bwd(B, Din, _p(dh), _p(w["Z"][i]), _p(dZ), _p(dZt), _p(self.gb[i - 1]),
-                                             st), "sur_act_bwd")
+                # dZ_{i-1} = (dZ_i . W_i) * SiLU'(Z_{i-1}), its transpose and bias gradient, one kernel
+                nxt = bufs[(i - 1) & 1].view(-1)[:B * Din].view(B, Din)
+                linear_silu_bwd(dz, self.Wt[i], w["Z"][i], nxt, dHt=dZt, db=self.gb[i - 1])
             elif want_dx:
                 gemm(dz, self.Wt[0], w["dX"])
         return w["loss"]
@@ -186,18 +212,13 @@ class Surrogate:
         The network's backward products without the weight gradients."""
         B = X.shape[0]
         w = self._work(B)
-        L = _lib.lib()
-        st = _st(self.device)
-        dZ = w["dZ"]
-        _lib.check(L.g1b_sur_seed(B * 64, _p(dY), _p(dZ), st), "sur_seed")
+        _lib.check(_lib.lib().g1b_sur_seed(B * 64, _p(dY), _p(w["dZ"]), _st(self.device)), "sur_seed")
+        bufs = [w["dZ"], w["dZ2"]]
         for i in range(4, -1, -1):
             Din, Dout = DIMS[i], DIMS[i + 1]
-            dz = dZ.view(-1)[:B * Dout].view(B, Dout)
+            dz = bufs[i & 1].view(-1)[:B * Dout].view(B, Dout)
             if i > 0:
-                dh = w["dH"].view(-1)[:B * Din].view(B, Din)
-                gemm(dz, self.Wt[i], dh)
-                _lib.check(L.g1b_sur_act_bwd(B, Din, _p(dh), _p(w["Z"][i]), _p(dZ), _p(w["dZt"]), _p(w["db"]), st),
-                           "sur_act_bwd")
+                linear_silu_bwd(dz, self.Wt[i], w["Z"][i], bufs[(i - 1) & 1].view(-1)[:B * Din].view(B, Din))
             else:
                 gemm(dz, self.Wt[0], w["dX"])
         return w["dX"]

@@ -245,21 +245,33 @@ int g1b_adjoint_noalloc(int nenv, const g1b_config* cfg, const g1b_adjoint_probl
 
 /* ------------------------------------------------- dynamics surrogate */
 /* No reference counterpart (the learned surrogate of the workload
- * configuration).  BF16 tcgen05 GEMM, FP32 accumulation:
+ * configuration).  BF16 tcgen05 GEMM, FP32 accumulation, persistent (one
+ * CTA per SM), operands loaded by TMA:
  *   C[M x N] = A[M x K] . B[N x K]^T (+ bias[N]), A, B row-major with K
- *   contiguous; splits > 1 splits K over CTAs and adds into C atomically
+ *   contiguous; splits > 1 splits K over tiles and adds into C atomically
  *   (C cleared first).  M % 128 == 0, N % 16 == 0 (N % 256 == 0 above 256),
- *   K % (64 splits) == 0, lda / ldb multiples of 8, ldc of 4. */
+ *   K % (64 splits) == 0, lda / ldb multiples of 8 and >= K, ldc a
+ *   multiple of 4 and >= N, 16-byte aligned pointers. */
 int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                   const float* bias, int splits, void* stream);
+/* One hidden layer of the surrogate in one GEMM with a fused epilogue
+ * (same shape rules; ldh a multiple of 8, ldz of 4, ldt >= M):
+ *   z = A . W^T + bias (W [N x K]); Z = z (FP32 [M][ldz], nullable),
+ *   H = bf16(silu(z)) [M][ldh], Ht = H transposed [N][ldt] (nullable). */
+int g1b_sur_linear_silu(int M, int N, int K, const void* A, int lda, const void* W, int ldw, const float* bias,
+                        float* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream);
+/* Its backward through the previous layer's activation: with Wt [N x K]
+ * (the layer's weight transposed) and Z [M][ldz] the previous layer's
+ * pre-activation, g = (dZ . Wt^T) * silu'(Z); dH = bf16(g) [M][ldh],
+ * dHt = dH transposed [N][ldt] (nullable), db[N] += column sums of g
+ * (FP32, nullable).  dH must not alias dZ. */
+int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const void* Wt, int ldw, const float* Z,
+                            int ldz, void* dH, int ldh, void* dHt, int ldt, float* db, void* stream);
 /* Device status of the GEMM kernels since the last call (synchronises):
  * 0 ok, 1 a pipeline wait timed out.  Clears the flag. */
 int g1b_gemm_status(int* code);
-/* Element-wise kernels of the surrogate: SiLU with transposed copy, its
- * backward with bias-gradient sums, weighted MSE and its gradient, Adam,
- * BF16 weight copies. */
-int g1b_sur_act(int B, int D, const float* Z, void* H, void* Ht, void* stream);
-int g1b_sur_act_bwd(int B, int D, const float* dH, const float* Z, void* dZ, void* dZt, float* db, void* stream);
+/* Element-wise kernels of the surrogate: weighted MSE and its gradient,
+ * Adam, BF16 weight copies. */
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream);
 int g1b_sur_adam(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,

@@ -66,6 +66,89 @@ def test_gemm_matches_fp64(M_, N, K, splits):
     assert err < 1e-5, err
 
 
+@pytest.mark.parametrize("M_,N,K,splits", [(20480, 512, 512, 1), (512, 192, 16384, 16)])
+def test_gemm_many_tiles_per_cta(M_, N, K, splits):
+    """More tiles than SMs: every CTA reuses both tensor-memory accumulators
+    and the operand ring several times (and, split, the atomic epilogue)."""
+    g = torch.Generator(device=DEV).manual_seed(M_ + N)
+    A = bf(torch.randn(M_, K, device=DEV, generator=g))
+    B = bf(torch.randn(N, K, device=DEV, generator=g))
+    C_ = torch.empty(M_, N, device=DEV)
+    S.gemm(A, B, C_, splits=splits)
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    ref = A.double() @ B.double().T
+    err = ((C_.double() - ref).norm() / ref.norm()).item()
+    assert err < 1e-5, err
+
+
+def _bf16_close(got, ref):
+    """got (BF16) is ref rounded to BF16, up to one unit in the last place
+    (the FP32 sums of the kernel and the FP64 reference may straddle a
+    rounding boundary), plus the FP32 accumulation error near zero."""
+    tol = ref.abs() * 2.0 ** -7 + 1e-5 * ref.abs().mean()
+    return bool(((got.double() - ref).abs() <= tol).all())
+
+
+@pytest.mark.parametrize("M_,N,K", [(256, 512, 512), (20480, 512, 512), (384, 192, 128), (128, 48, 64)])
+def test_linear_silu_fused_epilogue(M_, N, K):
+    """z = A W^T + b, H = bf16(silu(z)), Ht = H^T in one kernel, against FP64."""
+    g = torch.Generator(device=DEV).manual_seed(3 * M_ + N)
+    A = bf(torch.randn(M_, K, device=DEV, generator=g))
+    W = bf(torch.randn(N, K, device=DEV, generator=g) / K ** 0.5)
+    fence = torch.full((N + 64,), float("nan"), device=DEV)
+    fence[:N] = torch.randn(N, device=DEV, generator=g)
+    bias = fence[:N]
+    Z = torch.full((M_, N), 7.0, device=DEV)
+    H = torch.zeros(M_, N, dtype=torch.bfloat16, device=DEV)
+    Ht = torch.zeros(N, M_, dtype=torch.bfloat16, device=DEV)
+    S.linear_silu(A, W, bias, H, Z=Z, Ht=Ht)
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    zref = A.double() @ W.double().T + bias.double()
+    assert ((Z.double() - zref).norm() / zref.norm()).item() < 1e-5
+    assert _bf16_close(H, zref * torch.sigmoid(zref))
+    assert torch.equal(Ht, H.T)
+    # without the optional outputs: the same H
+    H2 = torch.zeros_like(H)
+    S.linear_silu(A, W, bias, H2)
+    torch.cuda.synchronize()
+    assert torch.equal(H2, H)
+
+
+@pytest.mark.parametrize("M_,N,K", [(256, 512, 512), (20480, 512, 512), (384, 192, 512), (128, 48, 64)])
+def test_linear_silu_bwd_fused_epilogue(M_, N, K):
+    """g = (dZ Wt^T) * silu'(Z), dH = bf16(g), dHt = dH^T, db += column sums of
+    g in one kernel, against FP64."""
+    g = torch.Generator(device=DEV).manual_seed(5 * M_ + N)
+    dZ = bf(torch.randn(M_, K, device=DEV, generator=g))
+    Wt = bf(torch.randn(N, K, device=DEV, generator=g) / K ** 0.5)
+    Z = torch.randn(M_, N, device=DEV, generator=g) * 2
+    dH = torch.zeros(M_, N, dtype=torch.bfloat16, device=DEV)
+    dHt = torch.zeros(N, M_, dtype=torch.bfloat16, device=DEV)
+    db = torch.full((N,), 0.25, device=DEV)
+    S.linear_silu_bwd(dZ, Wt, Z, dH, dHt=dHt, db=db)
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    z = Z.double()
+    s = torch.sigmoid(z)
+    gref = (dZ.double() @ Wt.double().T) * s * (1 + z * (1 - s))
+    assert _bf16_close(dH, gref)
+    assert torch.equal(dHt, dH.T)
+    dbref = gref.sum(0) + 0.25
+    assert ((db.double() - dbref).abs().max() / dbref.abs().max()).item() < 1e-5
+
+
+def test_linear_silu_rejects_aliasing_and_bad_shapes():
+    A = torch.zeros(128, 64, dtype=torch.bfloat16, device=DEV)
+    W = torch.zeros(64, 64, dtype=torch.bfloat16, device=DEV)
+    Z = torch.zeros(128, 64, device=DEV)
+    with pytest.raises(RuntimeError, match="alias"):
+        S.linear_silu_bwd(A, W, Z, A)
+    with pytest.raises(RuntimeError, match="M % 128"):
+        S.linear_silu(A[:96], W, None, torch.zeros(96, 64, dtype=torch.bfloat16, device=DEV))
+
+
 def cpu_reference(sur, X, T):
     """FP64 restatement of forward + weighted-MSE loss + backward with the
     kernels' BF16 rounding points (operands of every product)."""
