@@ -508,10 +508,12 @@ def adjoint_bench(device, stream, steps, warmup, world, n=ADJ_ENVS, horizon=ADJ_
             "finite": bool(torch.isfinite(r["grad_targets"]).all().item())}
 
 
-def measured_bf16_peak():
+def measured_bf16_peak(key="bf16_tflops"):
+    """A measured dense BF16 figure of this pool's B200s: the burst one, or
+    key="bf16_tflops_sustained" for work timed inside a long loop."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["bf16_tflops"])
+            return float(json.load(f)[key])
     except (OSError, KeyError, ValueError):
         return None
 
@@ -542,18 +544,23 @@ def surrogate_bench(device, train_steps, world):
     xt = xb.T.contiguous()
     sur.forward(xb, keep=True)
     l0 = float(sur.backward(xb, xt, tb).item())
-    # timed training steps (the same minibatch each step keeps the timed region to the kernels)
-    for _ in range(3):
-        sur.train_step(xb, xt, tb, lr=1e-3)
-    torch.cuda.synchronize()
+    # timed training steps (the same minibatch each step keeps the timed region to the kernels):
+    # the CUDA graph of the step the library's training loop replays, and the eager launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(10):
-        sur.train_step(xb, xt, tb, lr=1e-3)
-    e1.record()
-    torch.cuda.synchronize()
-    step_ms = e0.elapsed_time(e1) / 10
+    tg = sur.capture_train_step(xb, xt, tb, lr=1e-3)
+    timed = {}
+    for name, fn in (("graph", tg.step), ("eager", lambda: sur.train_step(xb, xt, tb, lr=1e-3))):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        timed[name] = e0.elapsed_time(e1) / 10
+    step_ms = timed["graph"]
     macs = sum(S.DIMS[i] * S.DIMS[i + 1] for i in range(5))
     train_tflops = 3 * 2 * SUR_BATCH * macs / (step_ms * 1e-3) / 1e12
     # inference throughput of the network alone (features in HBM)
@@ -563,15 +570,16 @@ def surrogate_bench(device, train_steps, world):
     e1.record()
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1) / 10
-    # the rest of the training budget on random minibatches
-    hist = []
+    # the rest of the training budget on random minibatches (gathered into the graph's buffers)
+    loss = None
     for k in range(train_steps):
         idx = torch.randint(0, X.shape[0], (SUR_BATCH,), generator=g, device=device)
-        xb = X[idx].contiguous()
-        lr = 2e-3 * (0.05 ** (k / max(train_steps, 1)))
-        hist.append(sur.train_step(xb, xb.T.contiguous(), T[idx].contiguous(), lr=lr))
+        torch.index_select(X, 0, idx, out=xb)
+        xt.copy_(xb.T)
+        torch.index_select(T, 0, idx, out=tb)
+        loss = tg.step(2e-3 * (0.05 ** (k / max(train_steps, 1))))
     torch.cuda.synchronize()
-    l1 = float(hist[-1].item()) if hist else l0
+    l1 = float(loss.item()) if loss is not None else l0
     from g1sim_b200 import workloads
     w = workloads.randomized(nenv=SUR_ENVS, seed=7)
     st = {k: torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("qpos", "qvel", "anchor", "ctrl")}
@@ -580,9 +588,10 @@ def surrogate_bench(device, train_steps, world):
     G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 20, DECIM, config=_cfg(), seed=7, mu=mu, dmass=dm)
     frac, err = S.rollout_with_fallback(sur, st, 50, bound=1e-3, mu=mu, dmass=dm)
     ref = refinement_bench(sur, device)
-    peak = measured_bf16_peak()
-    return {"train_step_ms": step_ms, "train_tflops": train_tflops,
+    peak, sustained = measured_bf16_peak(), measured_bf16_peak("bf16_tflops_sustained")
+    return {"train_step_ms": step_ms, "train_step_eager_ms": timed["eager"], "train_tflops": train_tflops,
             "train_frac_of_bf16_peak": (train_tflops / peak) if peak else None,
+            "train_frac_of_bf16_sustained": (train_tflops / sustained) if sustained else None,
             "bf16_peak_tflops": peak, "bf16_peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured",
             "train_flops_per_step": 3 * 2 * SUR_BATCH * macs,
             "inference": {"value": SUR_BATCH / (fwd_ms * 1e-3), "unit": "env-steps/s (network forward only)"},
@@ -660,9 +669,9 @@ def refinement_bench(sur, device, n=4096, H=50, iters=10):
 def gemm_bench(device, rows, steps, warmup):
     """The surrogate's layer products alone, rows x 512 x 512, each timed over
     `steps` calls with CUDA events: the plain product C = A W^T + b (FP32 C,
-    g1b_gemm_bf16), the fused hidden layer of training (FP32 Z, BF16 H and
-    H^T) and of inference (BF16 H only), the fused backward through SiLU (BF16
-    dZ and dZ^T, bias-gradient sums) and the weight gradient (K = rows split
+    g1b_gemm_bf16), the fused hidden layer of training (FP16 Z, BF16 H and
+    H^T) and of inference (BF16 H only), the fused backward through SiLU (FP16
+    Z in; BF16 dZ and dZ^T, bias-gradient sums) and the weight gradient (K = rows split
     over tiles, atomic FP32 sums).  hbm_gbs: algorithmic bytes (operands read
     once, outputs written once) per call over its time."""
     import torch
@@ -673,7 +682,7 @@ def gemm_bench(device, rows, steps, warmup):
     W = (torch.randn(512, 512, device=device, generator=g) / 512 ** 0.5).to(bf)
     b = torch.randn(512, device=device, generator=g)
     C_ = torch.empty(rows, 512, device=device)
-    Z = torch.randn(rows, 512, device=device, generator=g)
+    Z = torch.randn(rows, 512, device=device, generator=g).half()  # FP16 pre-activation
     H = torch.empty(rows, 512, dtype=bf, device=device)
     Ht = torch.empty(512, rows, dtype=bf, device=device)
     At = torch.randn(512, rows, device=device, generator=g).to(bf)
@@ -697,9 +706,9 @@ def gemm_bench(device, rows, steps, warmup):
     flops = 2.0 * rows * 512 * 512
     el = rows * 512
     cases = [("store", lambda: S.gemm(A_, W, C_, bias=b), el * (2 + 4)),
-             ("silu_forward_training", lambda: S.linear_silu(A_, W, b, H, Z=C_, Ht=Ht), el * (2 + 4 + 2 + 2)),
+             ("silu_forward_training", lambda: S.linear_silu(A_, W, b, H, Z=Z, Ht=Ht), el * (2 + 2 + 2 + 2)),
              ("silu_forward_inference", lambda: S.linear_silu(A_, W, b, H), el * (2 + 2)),
-             ("silu_backward", lambda: S.linear_silu_bwd(A_, W, Z, H, dHt=Ht, db=db), el * (2 + 4 + 2 + 2)),
+             ("silu_backward", lambda: S.linear_silu_bwd(A_, W, Z, H, dHt=Ht, db=db), el * (2 + 2 + 2 + 2)),
              ("weight_gradient", lambda: S.gemm(At, Ht, Cw, splits=splits), el * (2 + 2))]
     modes = {}
     for name, fn, nbytes in cases:

@@ -62,6 +62,12 @@ class AdjointProblem(C.Structure):
 _vp = C.c_void_p
 
 
+class SurLayer(C.Structure):
+    """g1b_sur_layer: one surrogate layer's parameters for g1b_sur_adam_cast."""
+    _fields_ = [(n, C.c_void_p) for n in ("W", "b", "mW", "vW", "mb", "vb", "gW", "gb", "Wb", "Wt")] + \
+        [("rows", C.c_int), ("cols", C.c_int)]
+
+
 def lib():
     """Load libg1cuda.so once and declare its signatures."""
     global _lib
@@ -98,7 +104,7 @@ def lib():
     L.g1b_sur_linear_silu_bwd.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,
                                                            _vp, C.c_int, _vp, _vp]
     L.g1b_sur_loss.argtypes = [C.c_int, C.c_int] + [_vp] * 8
-    L.g1b_sur_adam.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _vp]
+    L.g1b_sur_adam_cast.argtypes = [C.c_int, C.POINTER(SurLayer), _vp, _vp, C.c_float, C.c_float, C.c_float, _vp]
     L.g1b_sur_cast.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
     L.g1b_sur_features.argtypes = [C.c_int] + [_vp] * 12
     L.g1b_sur_features_vjp.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]

@@ -6,22 +6,26 @@
 //   contiguous, FP32 accumulation in tensor memory, and one of four
 //   epilogues (GemmMode):
 //     kGemmStore    C (FP32) = acc (+ bias)
-//     kGemmAtomic   C (FP32) += acc (+ bias on the first K split): K split
-//                   over tiles, C cleared by the caller
-//     kGemmSilu     z = acc + bias; Z (FP32, nullable) = z,
+//     kGemmAtomic   C (FP32) += acc (+ bias once): K split over CTAs
+//                   (stream-K), C cleared by the caller
+//     kGemmSilu     z = acc + bias; Z (FP16, nullable) = z,
 //                   H (BF16) = silu(z), Ht (BF16, transposed [N][M], nullable)
-//     kGemmSiluBwd  g = acc * silu'(Zin); H (BF16) = g, Ht = g transposed
-//                   (nullable), db[N] += column sums of g (nullable)
+//     kGemmSiluBwd  g = acc * silu'(Zin) (Zin FP16); H (BF16) = g, Ht = g
+//                   transposed (nullable), db[N] += column sums of g (nullable)
+// The pre-activation Z is kept in FP16 (11 significant bits, eight times
+// finer than the BF16 activations; |z| clamped to 65000, where silu' is
+// 0 or 1) only for the SiLU derivative of the backward pass.
 //
-// One CTA per SM (320 threads) walks the tiles blockIdx.x, + gridDim.x, ...
-// of 128 rows x Nt columns (Nt = min(N, 256)) and K split, row tiles
-// outermost so that the column tiles of one row block run close together
-// and read its A rows from L2.  Warp roles:
+// One CTA per SM (320 threads) walks its work units (GemmSched): tiles of
+// 128 rows x Nt columns (Nt = min(N, 256)), blockIdx.x, + gridDim.x, ...,
+// row tiles outermost so that the column tiles of one row block run close
+// together and read its A rows from L2; in the atomic mode an equal share of
+// (tile, K chunk) pairs per CTA.  Warp roles:
 //   warp 0   (one lane) TMA producer: for every 64-wide K chunk of a tile,
 //            waits until the MMAs have released the stage, then copies the
 //            A chunk (128 x 64) and the B chunk (Nt x 64) with
 //            cp.async.bulk.tensor (tensor maps over this GPU's memory, no
-//            multicast) into a kGemmStages-deep ring; the copies complete on
+//            multicast) into a 3-stage ring (4 in the atomic mode); the copies complete on
 //            the stage's `full` mbarrier (transaction bytes);
 //   warp 1   (one lane) MMA issuer: per chunk waits on `full`, issues four
 //            tcgen05.mma (M 128, N Nt, K 16) into one of two tensor-memory
@@ -60,38 +64,48 @@
 // released.
 //
 // Constraints (checked by the host launcher): M % 128 == 0, N % 16 == 0,
-// N % Nt == 0, K % (64 splits) == 0, lda / ldb / ldh / ldt multiples of 8,
+// N % Nt == 0, K % 64 == 0, lda / ldb / ldh / ldt multiples of 8,
 // ldc / ldz of 4, 16-byte aligned operands.
 
 constexpr int kGemmKC = 64;  // K columns per chunk (one 128-byte swizzle line)
 constexpr int kGemmMaxN = 256;
-constexpr int kGemmStages = 3;
+constexpr int kGemmMaxStages = 4;
 constexpr int kGemmEpiWarps = 8;  // two per TMEM lane quarter
 constexpr int kGemmThreads = 64 + 32 * kGemmEpiWarps;
 constexpr uint32_t kGemmABytes = 128 * kGemmKC * 2;        // 16 KB
 constexpr uint32_t kGemmBBytes = kGemmMaxN * kGemmKC * 2;  // 32 KB
 constexpr uint32_t kGemmStageBytes = kGemmABytes + kGemmBBytes;
 constexpr uint32_t kGemmAccCols = 256;  // one accumulator; two of them fill the 512 TMEM columns
-// Per epilogue warp one staging slot of: FP32 box 4 KB (output C / Z, or
-// the Z input), BF16 box 2 KB (H), transposed BF16 box 2 KB (Ht); and the
-// bias of its columns of the tile (128 floats).
+// Per epilogue warp one staging slot of: FP32 box 4 KB (output C) or FP16
+// box 2 KB (output Z, or the Z input), BF16 box 2 KB (H), transposed BF16
+// box 2 KB (Ht); and the bias of its columns of the tile (128 floats).
 constexpr uint32_t kEpiF = 0, kEpiH = 4096, kEpiT = 6144, kEpiWarpBytes = 8192, kEpiBiasBytes = 512;
-constexpr size_t kGemmSmem = kGemmStages * (size_t)kGemmStageBytes +
-                             kGemmEpiWarps * (size_t)(kEpiWarpBytes + kEpiBiasBytes) + 1024;
+// Operand ring depth: three stages next to the epilogue staging; four in the
+// atomic mode, whose epilogue adds straight into C and stages nothing (its
+// operands both stream from DRAM, so it needs the deeper ring most).
+template <int kMode>
+__host__ __device__ constexpr int gemm_stages() { return kMode == 1 ? 4 : 3; }
+template <int kMode>
+__host__ __device__ constexpr uint32_t gemm_epi_bytes() { return kMode == 1 ? 0u : kGemmEpiWarps * kEpiWarpBytes; }
+template <int kMode>
+__host__ __device__ constexpr size_t gemm_smem() {
+  return gemm_stages<kMode>() * (size_t)kGemmStageBytes + gemm_epi_bytes<kMode>() +
+         kGemmEpiWarps * (size_t)kEpiBiasBytes + 1024;
+}
 
 enum GemmMode : int { kGemmStore = 0, kGemmAtomic = 1, kGemmSilu = 2, kGemmSiluBwd = 3 };
 
 struct GemmArgs {
-  int ntm, ntn, splits, nk;  // row tiles, column tiles, K splits, chunks per split
+  int ntm, ntn, nk;  // row tiles, column tiles, 64-wide K chunks
   int Nt;                    // columns per tile
-  float* C;                  // store / atomic: C; silu: Z (nullable)
+  float* C;  // store / atomic: C
   int ldc;
   const float* bias;  // [N], nullable (store, atomic, silu)
   __nv_bfloat16* H;   // silu: silu(z); silu_bwd: g
   int ldh;
   __nv_bfloat16* Ht;  // transposed copy [N][ldt], nullable
   int ldt;
-  const float* Z;  // silu_bwd: the pre-activation
+  __half* Z;  // silu: the pre-activation out (nullable); silu_bwd: in
   int ldz;
   float* db;  // silu_bwd: column sums, nullable
   int* err;
@@ -99,7 +113,7 @@ struct GemmArgs {
 
 // The output tensor maps (a map the mode does not use holds a valid dummy).
 struct GemmOutMaps {
-  CUtensorMap f;  // FP32 [M][N] box 32 x 32, SWIZZLE_128B: C, Z (silu), Zin (silu_bwd)
+  CUtensorMap f;  // store: C, FP32 [M][N] box 32 x 32, SWIZZLE_128B; silu / silu_bwd: Z, FP16, SWIZZLE_64B
   CUtensorMap h;  // BF16 [M][N] box 32 x 32, SWIZZLE_64B: H
   CUtensorMap t;  // BF16 [N][M] box 32 x 32, no swizzle: Ht
 };
@@ -162,14 +176,43 @@ __device__ __forceinline__ bool gemm_wait(uint32_t bar, uint32_t parity, volatil
   return true;
 }
 
-struct GemmTile {
-  int m, n, sp;
+// One unit of a CTA's work: K chunks [k0, k0 + nk) of output tile (m, n).
+struct GemmWork {
+  int m, n, k0, nk;
 };
-__device__ __forceinline__ GemmTile gemm_tile(const GemmArgs& g, int t) {
-  const int per = g.ntm * g.ntn;
-  const int sp = t / per, r = t - sp * per;
-  return {r / g.ntn, r % g.ntn, sp};
-}
+// The CTA's sequence of work units (the producer, the MMA lane and the
+// epilogue walk the same one).  Atomic mode (stream-K): the CTA's contiguous
+// share [b T / G, (b + 1) T / G) of the T = tiles x K-chunks (tile, chunk)
+// pairs, cut at tile boundaries, so every SM gets the same number of chunks
+// whatever the tile count; partial tiles meet in C through the atomic adds.
+// Other modes: whole tiles blockIdx.x, + gridDim.x, ...
+template <int kMode>
+struct GemmSched {
+  int pos, end;
+  __device__ explicit GemmSched(const GemmArgs& g) {
+    if (kMode == kGemmAtomic) {
+      const long long T = (long long)g.ntm * g.ntn * g.nk;
+      pos = (int)(T * blockIdx.x / gridDim.x);
+      end = (int)(T * (blockIdx.x + 1) / gridDim.x);
+    } else {
+      pos = (int)blockIdx.x;
+      end = g.ntm * g.ntn;
+    }
+  }
+  __device__ bool next(const GemmArgs& g, GemmWork& w) {
+    if (pos >= end) return false;
+    if (kMode == kGemmAtomic) {
+      const int t = pos / g.nk, k0 = pos - t * g.nk;
+      const int nk = g.nk - k0 < end - pos ? g.nk - k0 : end - pos;
+      w = {t / g.ntn, t % g.ntn, k0, nk};
+      pos += nk;
+    } else {
+      w = {pos / g.ntn, pos % g.ntn, 0, g.nk};
+      pos += (int)gridDim.x;
+    }
+    return true;
+  }
+};
 
 // ------------------------------------------------------------ epilogue
 // Staging writes of one lane's row r (0..31) of a 32 x 32 box.
@@ -202,6 +245,33 @@ __device__ __forceinline__ void stage_bf16(uint8_t* box, int r, const float (&v)
     *reinterpret_cast<uint4*>(box + r * 64 + ((j ^ ((r >> 1) & 3)) << 4)) = w;
   }
 }
+// FP16 box, SWIZZLE_64B, as the BF16 one (the pre-activation Z).
+__device__ __forceinline__ void stage_f16(uint8_t* box, int r, const float (&v)[32]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const __half2 h = __floats2half2_rn(fminf(fmaxf(v[8 * j + 2 * i], -65000.0f), 65000.0f),
+                                          fminf(fmaxf(v[8 * j + 2 * i + 1], -65000.0f), 65000.0f));
+      w[i] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    *reinterpret_cast<uint4*>(box + r * 64 + ((j ^ ((r >> 1) & 3)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+__device__ __forceinline__ void unstage_f16(const uint8_t* box, int r, float (&v)[32]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint4 q = *reinterpret_cast<const uint4*>(box + r * 64 + ((j ^ ((r >> 1) & 3)) << 4));
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
+      v[8 * j + 2 * i] = f.x;
+      v[8 * j + 2 * i + 1] = f.y;
+    }
+  }
+}
 // Transposed BF16 box, no swizzle: element (column i, row r) at i * 64 + 2 r.
 __device__ __forceinline__ void stage_bf16_t(uint8_t* box, int r, const float (&v)[32]) {
   __nv_bfloat16* b = reinterpret_cast<__nv_bfloat16*>(box);
@@ -232,6 +302,11 @@ __device__ __forceinline__ void direct_f32(float* crow, const float (&v)[32], in
     else
       crow[i] = v[i];
   }
+}
+__device__ __forceinline__ void direct_f16(__half* zrow, const float (&v)[32], int nb) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i)
+    if (i < nb) zrow[i] = __float2half_rn(fminf(fmaxf(v[i], -65000.0f), 65000.0f));
 }
 __device__ __forceinline__ void direct_bf16(const GemmArgs& g, const float (&v)[32], int row, int col, int nb) {
   __nv_bfloat16* h = g.H + (size_t)row * g.ldh + col;
@@ -287,14 +362,16 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   const int par = ew >> 2;  // the warp's column groups: par, par + 2, ...
   uint8_t* const ep = ep0 + (size_t)ew * kEpiWarpBytes;
   const uint32_t es = ebase0 + (uint32_t)ew * kEpiWarpBytes;
-  float* const sbias = reinterpret_cast<float*>(ep0 + (size_t)kGemmEpiWarps * kEpiWarpBytes + ew * kEpiBiasBytes);
+  float* const sbias = reinterpret_cast<float*>(ep0 + gemm_epi_bytes<kMode>() + ew * kEpiBiasBytes);
   const uint32_t zb = tc::smem_u32(&zbar[ew]);
-  const bool st_f = kMode == kGemmStore || (kMode == kGemmSilu && g.C != nullptr);
+  const bool st_f = kMode == kGemmStore;                      // FP32 C
+  const bool st_z = kMode == kGemmSilu && g.Z != nullptr;      // FP16 Z
   const bool st_h = kMode == kGemmSilu || kMode == kGemmSiluBwd;
   const bool st_t = st_h && g.Ht != nullptr;
   const bool has_bias = g.bias != nullptr && kMode != kGemmSiluBwd;
   const int ngroups = (g.Nt + 31) / 32;
   const int spw = (ngroups - par + 1) / 2;  // this warp's groups per tile
+  // steps of the backward mode's Z prefetch (whole tiles blockIdx.x, + gridDim.x, ...)
   const int my_tiles = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int nsteps = my_tiles * spw;
   bool ok = true;
@@ -302,19 +379,21 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   // backward: TMA load of the Z box of step k (this warp's rows and group)
   auto z_issue = [&](int k) {
     if (lane == 0) {
-      const GemmTile tl = gemm_tile(g, (int)blockIdx.x + (k / spw) * (int)gridDim.x);
+      const int t = (int)blockIdx.x + (k / spw) * (int)gridDim.x;
       tc::fence_async_smem();
-      tc::mbar_expect_tx(zb, 4096);
-      tma_load_2d(es + kEpiF, mf, tl.n * g.Nt + (2 * (k % spw) + par) * 32, tl.m * 128 + q * 32, zb);
+      tc::mbar_expect_tx(zb, 2048);
+      tma_load_2d(es + kEpiF, mf, (t % g.ntn) * g.Nt + (2 * (k % spw) + par) * 32, (t / g.ntn) * 128 + q * 32, zb);
     }
     ++zi;
   };
   if (kMode == kGemmSiluBwd && nsteps > 0) z_issue(0);
   int k = 0, j = 0;
-  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++j) {
-    const GemmTile tl = gemm_tile(g, t);
+  GemmSched<kMode> sched(g);
+  GemmWork tl;
+  for (; ok && sched.next(g, tl); ++j) {
     const int b = j & 1;
-    if (has_bias && (kMode != kGemmAtomic || tl.sp == 0)) {  // this warp's bias values of the tile
+    const bool add_bias = has_bias && tl.k0 == 0;  // atomic mode: the unit holding K chunk 0
+    if (add_bias) {  // this warp's bias values of the tile
       __syncwarp();
       for (int s = 0; s < spw; ++s) {
         const int c = (2 * s + par) * 32 + lane;
@@ -343,13 +422,13 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
         }
         ++zw;
         float z[32];
-        unstage_f32(ep + kEpiF, lane, z);
+        unstage_f16(ep + kEpiF, lane, z);
         __syncwarp();  // every lane has read the box: the next one may land in its place
         if (k + 1 < nsteps) z_issue(k + 1);
 #pragma unroll
         for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
         if (g.db) column_sums(g.db, v, col, nb);
-      } else if (has_bias && (kMode != kGemmAtomic || tl.sp == 0)) {
+      } else if (add_bias) {
         const float4* bq = reinterpret_cast<const float4*>(sbias + s * 32);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -369,18 +448,20 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
       for (int i = 0; i < 32; ++i) hv[i] = kMode == kGemmSilu ? silu(v[i]) : v[i];
       if (nb < 32) {  // narrow group: plain stores
         if (st_f) direct_f32<false>(g.C + (size_t)row * g.ldc + col, v, nb);
+        if (st_z) direct_f16(g.Z + (size_t)row * g.ldz + col, v, nb);
         if (st_h) direct_bf16(g, hv, row, col, nb);
         continue;
       }
       if (lane == 0) bulk_wait_read0();  // the previous step's stores have read the slot
       __syncwarp();
       if (st_f) stage_f32(ep + kEpiF, lane, v);
+      if (st_z) stage_f16(ep + kEpiF, lane, v);
       if (st_h) stage_bf16(ep + kEpiH, lane, hv);
       if (st_t) stage_bf16_t(ep + kEpiT, lane, hv);
       tc::fence_async_smem();
       __syncwarp();
       if (lane == 0) {
-        if (st_f) tma_store_2d(mf, col, row0, es + kEpiF);
+        if (st_f || st_z) tma_store_2d(mf, col, row0, es + kEpiF);
         if (st_h) tma_store_2d(mh, col, row0, es + kEpiH);
         if (st_t) tma_store_2d(mt, row0, col, es + kEpiT);
         bulk_commit();
@@ -405,18 +486,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ GemmOutMaps om, GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t gsm[];
-  __shared__ uint64_t full[kGemmStages], empty[kGemmStages], accf[2], acce[2], drain, zbar[kGemmEpiWarps];
+  constexpr int kStages = gemm_stages<kMode>();
+  __shared__ uint64_t full[kStages], empty[kStages], accf[2], acce[2], drain, zbar[kGemmEpiWarps];
   __shared__ uint32_t tslot;
   __shared__ int abort_flag;
   volatile int* abort_v = &abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t base0 = tc::smem_u32(gsm);
   const uint32_t sbase = (base0 + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
-  const uint32_t ebase0 = sbase + (uint32_t)kGemmStages * kGemmStageBytes;  // epilogue staging
-  const int ntiles = g.ntm * g.ntn * g.splits;
+  const uint32_t ebase0 = sbase + (uint32_t)kStages * kGemmStageBytes;  // epilogue staging
+  const int ntiles = g.ntm * g.ntn;
   const uint32_t btx = (uint32_t)g.Nt * kGemmKC * 2;  // B bytes per chunk
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kGemmStages; ++s) {
+    for (int s = 0; s < kStages; ++s) {
       tc::mbar_init(tc::smem_u32(&full[s]), 1);
       tc::mbar_init(tc::smem_u32(&empty[s]), 1);
     }
@@ -441,27 +523,28 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
       asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
       uint32_t it = 0;  // chunks issued by this CTA
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const GemmTile tl = gemm_tile(g, t);
-        for (int c = 0; c < g.nk; ++c) {
-          const int s = (int)(it % kGemmStages);
-          const uint32_t r = it / kGemmStages;
+      GemmSched<kMode> sched(g);
+      GemmWork w;
+      while (ok && sched.next(g, w)) {
+        for (int c = 0; c < w.nk; ++c) {
+          const int s = (int)(it % kStages);
+          const uint32_t r = it / kStages;
           if (r > 0 && !gemm_wait(tc::smem_u32(&empty[s]), (r - 1) & 1, abort_v)) {
             ok = false;
             break;
           }
           const uint32_t st = sbase + (uint32_t)s * kGemmStageBytes;
           const uint32_t bar = tc::smem_u32(&full[s]);
-          const int kx = (tl.sp * g.nk + c) * kGemmKC;
+          const int kx = (w.k0 + c) * kGemmKC;
           tc::mbar_expect_tx(bar, kGemmABytes + btx);
-          tma_load_2d(st, &tmA, kx, tl.m * 128, bar);
-          tma_load_2d(st + kGemmABytes, &tmB, kx, tl.n * g.Nt, bar);
+          tma_load_2d(st, &tmA, kx, w.m * 128, bar);
+          tma_load_2d(st + kGemmABytes, &tmB, kx, w.n * g.Nt, bar);
           ++it;
         }
       }
       // every copy issued has landed before the CTA may exit
-      for (int s = 0; s < kGemmStages; ++s) {
-        const uint32_t n_s = it > (uint32_t)s ? (it - (uint32_t)s - 1) / kGemmStages + 1 : 0;
+      for (int s = 0; s < kStages; ++s) {
+        const uint32_t n_s = it > (uint32_t)s ? (it - (uint32_t)s - 1) / kStages + 1 : 0;
         if (n_s > 0 && !tc::mbar_wait(tc::smem_u32(&full[s]), (n_s - 1) & 1)) ok = false;
       }
     }
@@ -469,8 +552,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (lane == 0) {  // ---- MMA issuer
       const uint32_t idesc = tc::idesc_bf16(128, g.Nt);
       uint32_t it = 0;
-      int j = 0;  // tiles of this CTA
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++j) {
+      int j = 0;  // work units of this CTA
+      GemmSched<kMode> sched(g);
+      GemmWork w;
+      for (; ok && sched.next(g, w); ++j) {
         const int b = j & 1;
         const uint32_t u = (uint32_t)j >> 1;
         if (u > 0 && !gemm_wait(tc::smem_u32(&acce[b]), (u - 1) & 1, abort_v)) {
@@ -479,9 +564,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         }
         tc::tc_fence_after();
         const uint32_t d = tmem + (uint32_t)b * kGemmAccCols;
-        for (int c = 0; c < g.nk; ++c, ++it) {
-          const int s = (int)(it % kGemmStages);
-          const uint32_t r = it / kGemmStages;
+        for (int c = 0; c < w.nk; ++c, ++it) {
+          const int s = (int)(it % kStages);
+          const uint32_t r = it / kStages;
           if (!gemm_wait(tc::smem_u32(&full[s]), r & 1, abort_v)) {
             ok = false;
             break;

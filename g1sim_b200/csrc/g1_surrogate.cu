@@ -4,10 +4,12 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
 
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -56,13 +58,11 @@ static int map_bf16_operand(CUtensorMap* m, const void* p, int rows, int cols, i
 // (one CTA per SM, at most one per tile).
 template <int kMode>
 static int gemm_run(const char* what, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
-                    int splits, GemmArgs g, cudaStream_t st, bool clear_c = false) {
+                    GemmArgs g, cudaStream_t st, bool clear_c = false) {
   if (M <= 0 || N <= 0 || K <= 0 || !A || !B) return failf("%s: invalid arguments", what);
-  if (splits < 1) splits = 1;
   const int Nt = N <= kGemmMaxN ? N : kGemmMaxN;
-  if (M % 128 || N % 16 || N % Nt || K % (kGemmKC * splits))
-    return failf("%s: needs M %% 128 == 0, N %% 16 == 0 (and N %% 256 == 0 above 256), K %% (64 splits) == 0",
-                 what);
+  if (M % 128 || N % 16 || N % Nt || K % kGemmKC)
+    return failf("%s: needs M %% 128 == 0, N %% 16 == 0 (and N %% 256 == 0 above 256), K %% 64 == 0", what);
   if (lda % 8 || ldb % 8 || lda < K || ldb < K || (((uintptr_t)A | (uintptr_t)B) & 15))
     return failf("%s: lda, ldb multiples of 8 and >= K, 16-byte aligned operands", what);
   if (g.Ht && (g.ldt % 8 || ((uintptr_t)g.Ht & 15)))
@@ -71,10 +71,12 @@ static int gemm_run(const char* what, int M, int N, int K, const void* A, int ld
   GemmOutMaps om;
   memset(&om, 0, sizeof(om));
   if (map_bf16_operand(&ma, A, M, K, lda, 128) || map_bf16_operand(&mb, B, N, K, ldb, Nt)) return -1;
-  const float* fsrc = kMode == kGemmSiluBwd ? g.Z : g.C;  // FP32 box: C, Z out, or Z in
-  const int fld = kMode == kGemmSiluBwd ? g.ldz : g.ldc;
-  if (fsrc && kMode != kGemmAtomic &&
-      gemm_map(&om.f, fsrc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, M, N, fld, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B))
+  // the f map: FP32 C (store), or the FP16 pre-activation (silu out, silu_bwd in)
+  if (kMode == kGemmStore &&
+      gemm_map(&om.f, g.C, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, M, N, g.ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B))
+    return -1;
+  if ((kMode == kGemmSilu || kMode == kGemmSiluBwd) && g.Z &&
+      gemm_map(&om.f, g.Z, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, M, N, g.ldz, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B))
     return -1;
   if (g.H && gemm_map(&om.h, g.H, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, M, N, g.ldh, 32, 32,
                       CU_TENSOR_MAP_SWIZZLE_64B))
@@ -88,17 +90,18 @@ static int gemm_run(const char* what, int M, int N, int K, const void* A, int ld
     return cuda_fail(e, "gemm: clear C");
   g.ntm = M / 128;
   g.ntn = N / Nt;
-  g.splits = splits;
-  g.nk = K / (kGemmKC * splits);
+  g.nk = K / kGemmKC;
   g.Nt = Nt;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int ntiles = g.ntm * g.ntn * splits;
-  const int grid = ntiles < sms ? ntiles : sms;
-  if ((e = prepare<20, kMode>(gemm_kernel<kMode>, kGemmSmem)) != cudaSuccess)
+  // work items: whole tiles, or (atomic, stream-K) (tile, K chunk) pairs shared evenly by the CTAs
+  const long long units = (long long)g.ntm * g.ntn * (kMode == kGemmAtomic ? g.nk : 1);
+  if (units > INT32_MAX) return failf("%s: problem too large", what);
+  const int grid = units < sms ? (int)units : sms;
+  if ((e = prepare<20, kMode>(gemm_kernel<kMode>, gemm_smem<kMode>())) != cudaSuccess)
     return cuda_fail(e, "gemm: attributes");
-  gemm_kernel<kMode><<<grid, kGemmThreads, kGemmSmem, st>>>(ma, mb, om, g);
+  gemm_kernel<kMode><<<grid, kGemmThreads, gemm_smem<kMode>(), st>>>(ma, mb, om, g);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : cuda_fail(e, "gemm_kernel");
 }
@@ -115,32 +118,32 @@ int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
   g.C = C;
   g.ldc = ldc;
   g.bias = bias;
-  if (splits > 1) return gemm_run<kGemmAtomic>("gemm_bf16", M, N, K, A, lda, B, ldb, splits, g, st, true);
-  return gemm_run<kGemmStore>("gemm_bf16", M, N, K, A, lda, B, ldb, 1, g, st);
+  if (splits > 1) return gemm_run<kGemmAtomic>("gemm_bf16", M, N, K, A, lda, B, ldb, g, st, true);
+  return gemm_run<kGemmStore>("gemm_bf16", M, N, K, A, lda, B, ldb, g, st);
 }
 
 int g1b_sur_linear_silu(int M, int N, int K, const void* A, int lda, const void* W, int ldw, const float* bias,
-                        float* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream) {
+                        void* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream) {
   if (!H || ldh < N || ldh % 8 || ((uintptr_t)H & 15))
     return fail("sur_linear_silu: H needs ldh >= N, ldh % 8 == 0, 16-byte alignment");
-  if (Z && (ldz < N || ldz % 4 || ((uintptr_t)Z & 15)))
-    return fail("sur_linear_silu: Z needs ldz >= N, ldz % 4 == 0, 16-byte alignment");
+  if (Z && (ldz < N || ldz % 8 || ((uintptr_t)Z & 15)))
+    return fail("sur_linear_silu: Z needs ldz >= N, ldz % 8 == 0, 16-byte alignment");
   if (Ht && ldt < M) return fail("sur_linear_silu: Ht needs ldt >= M");
   GemmArgs g{};
-  g.C = Z;
-  g.ldc = ldz;
+  g.Z = static_cast<__half*>(Z);
+  g.ldz = ldz;
   g.bias = bias;
   g.H = static_cast<__nv_bfloat16*>(H);
   g.ldh = ldh;
   g.Ht = static_cast<__nv_bfloat16*>(Ht);
   g.ldt = ldt;
-  return gemm_run<kGemmSilu>("sur_linear_silu", M, N, K, A, lda, W, ldw, 1, g, static_cast<cudaStream_t>(stream));
+  return gemm_run<kGemmSilu>("sur_linear_silu", M, N, K, A, lda, W, ldw, g, static_cast<cudaStream_t>(stream));
 }
 
-int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const void* W, int ldw, const float* Z,
+int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const void* W, int ldw, const void* Z,
                             int ldz, void* dH, int ldh, void* dHt, int ldt, float* db, void* stream) {
-  if (!Z || ldz < N || ldz % 4 || ((uintptr_t)Z & 15))
-    return fail("sur_linear_silu_bwd: Z needs ldz >= N, ldz % 4 == 0, 16-byte alignment");
+  if (!Z || ldz < N || ldz % 8 || ((uintptr_t)Z & 15))
+    return fail("sur_linear_silu_bwd: Z needs ldz >= N, ldz % 8 == 0, 16-byte alignment");
   if (!dH || ldh < N || ldh % 8 || ((uintptr_t)dH & 15))
     return fail("sur_linear_silu_bwd: dH needs ldh >= N, ldh % 8 == 0, 16-byte alignment");
   if (dHt && ldt < M) return fail("sur_linear_silu_bwd: dHt needs ldt >= M");
@@ -150,11 +153,10 @@ int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const 
   g.ldh = ldh;
   g.Ht = static_cast<__nv_bfloat16*>(dHt);
   g.ldt = ldt;
-  g.Z = Z;
+  g.Z = const_cast<__half*>(static_cast<const __half*>(Z));
   g.ldz = ldz;
   g.db = db;
-  return gemm_run<kGemmSiluBwd>("sur_linear_silu_bwd", M, N, K, dZ, ldd, W, ldw, 1, g,
-                                static_cast<cudaStream_t>(stream));
+  return gemm_run<kGemmSiluBwd>("sur_linear_silu_bwd", M, N, K, dZ, ldd, W, ldw, g, static_cast<cudaStream_t>(stream));
 }
 
 int g1b_gemm_status(int* code) {
@@ -182,13 +184,30 @@ int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, v
   return launched("sur_loss_kernel");
 }
 
-int g1b_sur_adam(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
-                 int step, void* stream) {
-  if (n <= 0 || !p || !g || !m || !v || step < 1) return fail("sur_adam: invalid arguments");
-  const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
-  sur_adam_kernel<<<grid_1d((size_t)n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(n, p, g, m, v, lr, b1, b2,
-                                                                                         eps, c1, c2);
-  return launched("sur_adam_kernel");
+int g1b_sur_adam_cast(int nl, const g1b_sur_layer* layers, const int* step, const float* lr, float b1, float b2,
+                      float eps, void* stream) {
+  if (nl <= 0 || nl > kSurMaxLayers || !layers || !step || !lr) return fail("sur_adam_cast: invalid arguments");
+  SurOpt o{};
+  long long total = 0;
+  for (int i = 0; i < nl; ++i) {
+    const g1b_sur_layer& L = layers[i];
+    if (!L.W || !L.b || !L.mW || !L.vW || !L.mb || !L.vb || !L.gW || !L.gb || !L.Wb || !L.Wt || L.rows <= 0 ||
+        L.cols <= 0)
+      return fail("sur_adam_cast: invalid layer");
+    o.l[i] = {L.W, L.b, L.mW, L.vW, L.mb, L.vb, L.gW, L.gb, static_cast<__nv_bfloat16*>(L.Wb),
+              static_cast<__nv_bfloat16*>(L.Wt), L.rows, L.cols};
+    total += (long long)L.rows * L.cols + L.rows;
+  }
+  if (total > INT32_MAX) return fail("sur_adam_cast: too many parameters");
+  o.nl = nl;
+  o.total = (int)total;
+  o.step = step;
+  o.lr = lr;
+  o.b1 = b1;
+  o.b2 = b2;
+  o.eps = eps;
+  sur_adam_cast_kernel<<<grid_1d((size_t)total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(o);
+  return launched("sur_adam_cast_kernel");
 }
 
 int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* stream) {

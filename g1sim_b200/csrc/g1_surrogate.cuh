@@ -67,15 +67,60 @@ __global__ void sur_loss_kernel(int B, int D, const float* __restrict__ Y, const
 }
 
 // Adam (Kingma & Ba 2015) with bias correction, in place on FP32 p, m, v.
-__global__ void sur_adam_kernel(int n, float* p, const float* __restrict__ g, float* m, float* v, float lr, float b1,
-                                float b2, float eps, float c1, float c2) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+// The optimiser step of every layer in one launch: Adam on the FP32
+// weights and biases (moments m, v; bias corrections 1 - b1^t, 1 - b2^t for
+// the step count t and the learning rate read from device memory, so that a
+// captured CUDA graph of the training step replays with the current ones),
+// then the BF16 copy and BF16 transpose of each updated weight that the
+// GEMMs read.  Thread i owns the i-th entry of the layers' weights and
+// biases taken in order.
+struct SurLayerOpt {
+  float *W, *b, *mW, *vW, *mb, *vb;
+  const float *gW, *gb;
+  __nv_bfloat16 *Wb, *Wt;
+  int rows, cols;
+};
+constexpr int kSurMaxLayers = 8;
+struct SurOpt {
+  SurLayerOpt l[kSurMaxLayers];
+  int nl, total;
+  const int* step;
+  const float* lr;
+  float b1, b2, eps;
+};
+
+__device__ __forceinline__ float adam_update(float& p, float& m, float& v, float g, float lr, float b1, float b2,
+                                             float eps, float c1, float c2) {
+  const float mi = b1 * m + (1.0f - b1) * g;
+  const float vi = b2 * v + (1.0f - b2) * g * g;
+  m = mi;
+  v = vi;
+  p -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  return p;
+}
+
+__global__ void sur_adam_cast_kernel(SurOpt o) {
+  const float t = (float)*o.step, lr = *o.lr;
+  const float c1 = 1.0f - powf(o.b1, t), c2 = 1.0f - powf(o.b2, t);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.total; i += gridDim.x * blockDim.x) {
+    int k = i;
+    for (int L = 0; L < o.nl; ++L) {
+      const SurLayerOpt& q = o.l[L];
+      const int nw = q.rows * q.cols;
+      if (k < nw) {
+        const float p = adam_update(q.W[k], q.mW[k], q.vW[k], q.gW[k], lr, o.b1, o.b2, o.eps, c1, c2);
+        const __nv_bfloat16 h = __float2bfloat16_rn(p);
+        q.Wb[k] = h;
+        q.Wt[(size_t)(k % q.cols) * q.rows + k / q.cols] = h;
+        break;
+      }
+      k -= nw;
+      if (k < q.rows) {
+        adam_update(q.b[k], q.mb[k], q.vb[k], q.gb[k], lr, o.b1, o.b2, o.eps, c1, c2);
+        break;
+      }
+      k -= q.rows;
+    }
   }
 }
 

@@ -62,11 +62,12 @@ def gemm(A, B, C_, bias=None, splits=1):
 
 def linear_silu(A, W, bias, H, Z=None, Ht=None):
     """One hidden layer, fused: z = A @ W^T + bias; H = bf16(silu(z)) [M, N];
-    Z = z (FP32 [M, N], optional); Ht = H^T ([N, M] BF16, optional)."""
+    Z = z (FP16 [M, N], optional: the backward pass's SiLU derivative);
+    Ht = H^T ([N, M] BF16, optional)."""
     M_, K = A.shape
     N = W.shape[0]
     assert W.shape[1] == K and H.shape == (M_, N) and A.dtype == W.dtype == torch.bfloat16
-    assert Z is None or Z.shape == (M_, N)
+    assert Z is None or (Z.shape == (M_, N) and Z.dtype == torch.float16)
     assert Ht is None or (Ht.shape[0] == N and Ht.shape[1] >= M_)
     _lib.check(_lib.lib().g1b_sur_linear_silu(M_, N, K, _p(A), A.stride(0), _p(W), W.stride(0), _p(bias), _p(Z),
                                               Z.stride(0) if Z is not None else 0, _p(H), H.stride(0), _p(Ht),
@@ -76,11 +77,12 @@ def linear_silu(A, W, bias, H, Z=None, Ht=None):
 
 def linear_silu_bwd(dZ, Wt, Z, dH, dHt=None, db=None):
     """Backward through a layer and the previous activation, fused:
-    g = (dZ @ Wt^T) * silu'(Z); dH = bf16(g) [M, N]; dHt = dH^T (optional);
+    g = (dZ @ Wt^T) * silu'(Z) (Z FP16); dH = bf16(g) [M, N]; dHt = dH^T (optional);
     db += column sums of g (optional).  dH must not share memory with dZ."""
     M_, K = dZ.shape
     N = Wt.shape[0]
     assert Wt.shape[1] == K and dH.shape == (M_, N) and Z.shape[0] == M_ and Z.shape[1] >= N
+    assert Z.dtype == torch.float16
     assert dHt is None or (dHt.shape[0] == N and dHt.shape[1] >= M_)
     _lib.check(_lib.lib().g1b_sur_linear_silu_bwd(M_, N, K, _p(dZ), dZ.stride(0), _p(Wt), Wt.stride(0), _p(Z),
                                                   Z.stride(0), _p(dH), dH.stride(0), _p(dHt),
@@ -119,6 +121,14 @@ class Surrogate:
         self.gW = [torch.zeros(max(w.shape[0], 128), w.shape[1], device=device) for w in self.W]
         self.gb = [torch.zeros_like(b) for b in self.b]
         self.step_n = 0
+        # Adam's step count and learning rate live on the device, so that a
+        # CUDA graph of the training step replays with the current ones
+        self.opt_step = torch.zeros(1, dtype=torch.int32, device=device)
+        self.lr_dev = torch.full((1,), 1e-3, device=device)
+        self._layers = (_lib.SurLayer * 5)(*[
+            _lib.SurLayer(*[t.data_ptr() for t in (self.W[i], self.b[i], self.mW[i], self.vW[i], self.mb[i],
+                                                    self.vb[i], self.gW[i], self.gb[i], self.Wb[i], self.Wt[i])],
+                          self.W[i].shape[0], self.W[i].shape[1]) for i in range(5)])
         self.in_mean = torch.zeros(NIN, device=device)
         self.in_istd = torch.ones(NIN, device=device)
         self.out_mean = torch.zeros(64, device=device)
@@ -137,7 +147,9 @@ class Surrogate:
         if B not in self._ws:
             d, bf = self.device, torch.bfloat16
             self._ws[B] = dict(
-                Z=[None] + [torch.empty(B, DIMS[i], device=d) for i in range(1, 6)],
+                # pre-activations: FP16 for the hidden layers (their SiLU derivative), FP32 output
+                Z=[None] + [torch.empty(B, DIMS[i], dtype=torch.float16, device=d) for i in range(1, 5)] +
+                  [torch.empty(B, DIMS[5], device=d)],
                 H=[None] + [torch.empty(B, DIMS[i], dtype=bf, device=d) for i in range(1, 5)],
                 Ht=[None] + [torch.empty(DIMS[i], B, dtype=bf, device=d) for i in range(1, 5)],
                 dX=torch.empty(B, NIN, device=d),
@@ -224,16 +236,15 @@ class Surrogate:
         return w["dX"]
 
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        """One Adam step of every layer and the BF16 weight copies, one launch.
+        lr: the learning rate, written to the device first (None: keep the
+        device's; the form a captured graph uses)."""
+        if lr is not None:
+            self.lr_dev.fill_(lr)
+        self.opt_step.add_(1)
         self.step_n += 1
-        L = _lib.lib()
-        st = _st(self.device)
-        for i in range(5):
-            gw = self.gW[i][:self.W[i].shape[0]]  # leading rows: contiguous
-            _lib.check(L.g1b_sur_adam(self.W[i].numel(), _p(self.W[i]), _p(gw),
-                                      _p(self.mW[i]), _p(self.vW[i]), lr, b1, b2, eps, self.step_n, st), "sur_adam")
-            _lib.check(L.g1b_sur_adam(self.b[i].numel(), _p(self.b[i]), _p(self.gb[i]), _p(self.mb[i]),
-                                      _p(self.vb[i]), lr, b1, b2, eps, self.step_n, st), "sur_adam")
-        self.cast()
+        _lib.check(_lib.lib().g1b_sur_adam_cast(5, self._layers, _p(self.opt_step), _p(self.lr_dev), b1, b2, eps,
+                                                _st(self.device)), "sur_adam_cast")
 
     def train_step(self, X, Xt, T, lr=1e-3):
         self.forward(X, keep=True)
@@ -241,10 +252,44 @@ class Surrogate:
         self.adam(lr)
         return loss
 
+    def capture_train_step(self, X, Xt, T, lr):
+        """A CUDA graph of train_step on the fixed buffers X, Xt, T (write the
+        next minibatch into them, then call the returned step(lr)).  Runs one
+        eager training step first (with `lr`), which prepares every kernel."""
+        return TrainGraph(self, X, Xt, T, lr)
+
     def integrate(self, Y, qpos, qvel, dt):
         n = qpos.shape[1]
         _lib.check(_lib.lib().g1b_sur_integrate(n, _p(Y), Y.stride(0), _p(self.out_mean), _p(self.out_std), dt,
                                                  _p(qpos), _p(qvel), _st(self.device)), "sur_integrate")
+
+
+class TrainGraph:
+    """One surrogate training step (forward, loss, backward, Adam) captured as
+    a CUDA graph on fixed input buffers: the ~25 launches of a step replay
+    without the host in between.  The learning rate and Adam's step count are
+    read from device memory, so each replay uses the current ones."""
+
+    def __init__(self, sur, X, Xt, T, lr):
+        self.sur = sur
+        dev = sur.device
+        s = torch.cuda.Stream(dev)
+        s.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(s):
+            sur.train_step(X, Xt, T, lr=lr)  # a real step, which also prepares the kernels
+        torch.cuda.current_stream(dev).wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=s):
+            self.loss = sur.train_step(X, Xt, T, lr=None)
+        sur.step_n -= 1  # the capture ran no step
+
+    def step(self, lr=None):
+        """One training step; returns the (device) loss buffer."""
+        if lr is not None:
+            self.sur.lr_dev.fill_(lr)
+        self.graph.replay()
+        self.sur.step_n += 1
+        return self.loss
 
 
 # ------------------------------------------------------------- data
@@ -314,18 +359,28 @@ def normalise(sur, F, A=None):
 
 
 def train(sur, F, A, steps, batch=65536, lr=1e-3, seed=0, log_every=0):
-    """Minibatch training on the library's kernels; returns the loss history."""
+    """Minibatch training on the library's kernels; returns the loss history.
+    Each minibatch is gathered into fixed buffers and the step replayed as a
+    CUDA graph (the first step runs eagerly and captures it)."""
     X, T = normalise(sur, F, A)
     N = X.shape[0]
-    g = torch.Generator(device=X.device).manual_seed(seed)
-    hist = []
+    dev = X.device
+    g = torch.Generator(device=dev).manual_seed(seed)
+    xb = torch.empty(batch, NIN, dtype=torch.bfloat16, device=dev)
+    xt = torch.empty(NIN, batch, dtype=torch.bfloat16, device=dev)
+    tb = torch.empty(batch, T.shape[1], device=dev)
+    hist, tg = [], None
     for k in range(steps):
-        idx = torch.randint(0, N, (batch,), generator=g, device=X.device)
-        xb = X[idx].contiguous()
-        xt = xb.T.contiguous()
-        tb = T[idx].contiguous()
+        idx = torch.randint(0, N, (batch,), generator=g, device=dev)
+        torch.index_select(X, 0, idx, out=xb)
+        xt.copy_(xb.T)
+        torch.index_select(T, 0, idx, out=tb)
         cur_lr = lr * (0.1 ** (k / max(steps, 1)))
-        loss = sur.train_step(xb, xt, tb, lr=cur_lr)
+        if tg is None:
+            tg = sur.capture_train_step(xb, xt, tb, cur_lr)
+            loss = tg.loss
+        else:
+            loss = tg.step(cur_lr)
         if log_every and k % log_every == 0:
             hist.append((k, float(loss.item())))
     return hist

@@ -248,34 +248,49 @@ int g1b_adjoint_noalloc(int nenv, const g1b_config* cfg, const g1b_adjoint_probl
  * configuration).  BF16 tcgen05 GEMM, FP32 accumulation, persistent (one
  * CTA per SM), operands loaded by TMA:
  *   C[M x N] = A[M x K] . B[N x K]^T (+ bias[N]), A, B row-major with K
- *   contiguous; splits > 1 splits K over tiles and adds into C atomically
- *   (C cleared first).  M % 128 == 0, N % 16 == 0 (N % 256 == 0 above 256),
- *   K % (64 splits) == 0, lda / ldb multiples of 8 and >= K, ldc a
- *   multiple of 4 and >= N, 16-byte aligned pointers. */
+ *   contiguous; splits > 1 selects the K-split form for small outputs of
+ *   long products: the (tile, 64-wide K chunk) pairs are shared evenly by
+ *   the SMs and their partial tiles added into C atomically (C cleared
+ *   first; the sum order, and so the last bits, vary from call to call).
+ *   M % 128 == 0, N % 16 == 0 (N % 256 == 0 above 256), K % 64 == 0,
+ *   lda / ldb multiples of 8 and >= K, ldc a multiple of 4 and >= N,
+ *   16-byte aligned pointers. */
 int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                   const float* bias, int splits, void* stream);
 /* One hidden layer of the surrogate in one GEMM with a fused epilogue
- * (same shape rules; ldh a multiple of 8, ldz of 4, ldt >= M):
- *   z = A . W^T + bias (W [N x K]); Z = z (FP32 [M][ldz], nullable),
- *   H = bf16(silu(z)) [M][ldh], Ht = H transposed [N][ldt] (nullable). */
+ * (same shape rules; ldh and ldz multiples of 8, ldt >= M):
+ *   z = A . W^T + bias (W [N x K]); Z = z (FP16 [M][ldz], |z| clamped to
+ *   65000, nullable), H = bf16(silu(z)) [M][ldh], Ht = H transposed
+ *   [N][ldt] (nullable). */
 int g1b_sur_linear_silu(int M, int N, int K, const void* A, int lda, const void* W, int ldw, const float* bias,
-                        float* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream);
+                        void* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream);
 /* Its backward through the previous layer's activation: with Wt [N x K]
- * (the layer's weight transposed) and Z [M][ldz] the previous layer's
- * pre-activation, g = (dZ . Wt^T) * silu'(Z); dH = bf16(g) [M][ldh],
- * dHt = dH transposed [N][ldt] (nullable), db[N] += column sums of g
- * (FP32, nullable).  dH must not alias dZ. */
-int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const void* Wt, int ldw, const float* Z,
+ * (the layer's weight transposed) and Z [M][ldz] (FP16) the previous
+ * layer's pre-activation, g = (dZ . Wt^T) * silu'(Z); dH = bf16(g)
+ * [M][ldh], dHt = dH transposed [N][ldt] (nullable), db[N] += column sums
+ * of g (FP32, nullable).  dH must not alias dZ. */
+int g1b_sur_linear_silu_bwd(int M, int N, int K, const void* dZ, int ldd, const void* Wt, int ldw, const void* Z,
                             int ldz, void* dH, int ldh, void* dHt, int ldt, float* db, void* stream);
 /* Device status of the GEMM kernels since the last call (synchronises):
  * 0 ok, 1 a pipeline wait timed out.  Clears the flag. */
 int g1b_gemm_status(int* code);
+/* The optimiser step of the surrogate in one launch: Adam (b1, b2, eps;
+ * the step count t and the learning rate read from device memory, t >= 1)
+ * on every layer's FP32 weights and biases with their gradients gW
+ * (leading rows x cols entries) and gb, then the BF16 copies Wb [rows][cols]
+ * and Wt [cols][rows] of each updated weight.  At most 8 layers. */
+typedef struct g1b_sur_layer {
+  float *W, *b, *mW, *vW, *mb, *vb;
+  const float *gW, *gb;
+  void *Wb, *Wt;
+  int rows, cols;
+} g1b_sur_layer;
+int g1b_sur_adam_cast(int nl, const g1b_sur_layer* layers, const int* step, const float* lr, float b1, float b2,
+                      float eps, void* stream);
 /* Element-wise kernels of the surrogate: weighted MSE and its gradient,
- * Adam, BF16 weight copies. */
+ * BF16 weight copies. */
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream);
-int g1b_sur_adam(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
-                 int step, void* stream);
 int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* stream);
 /* The surrogate's input features of n envs (159 used of 192: joint angles
  * and rates, base height, rotation, body-frame velocities, per foot sphere
