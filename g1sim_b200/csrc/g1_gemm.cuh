@@ -155,8 +155,9 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int 
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// No committed group of this thread still reading shared memory.
+// No committed group of this thread still reading shared memory / at most the last one.
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 // Every committed group of this thread complete.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void gemm_arrive(uint32_t bar) {
@@ -363,7 +364,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   uint8_t* const ep = ep0 + (size_t)ew * kEpiWarpBytes;
   const uint32_t es = ebase0 + (uint32_t)ew * kEpiWarpBytes;
   float* const sbias = reinterpret_cast<float*>(ep0 + gemm_epi_bytes<kMode>() + ew * kEpiBiasBytes);
-  const uint32_t zb = tc::smem_u32(&zbar[ew]);
+  const uint32_t zb0 = tc::smem_u32(&zbar[2 * ew]);  // Z box k in slot k % 2: barrier zb0 + 8 (k % 2)
   const bool st_f = kMode == kGemmStore;                      // FP32 C
   const bool st_z = kMode == kGemmSilu && g.Z != nullptr;      // FP16 Z
   const bool st_h = kMode == kGemmSilu || kMode == kGemmSiluBwd;
@@ -375,18 +376,21 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   const int my_tiles = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int nsteps = my_tiles * spw;
   bool ok = true;
-  int zi = 0, zw = 0;  // backward: Z boxes issued, waited for
+  int zi = 0, zw = 0;  // backward: Z boxes issued, waited for (two in flight)
   // backward: TMA load of the Z box of step k (this warp's rows and group)
   auto z_issue = [&](int k) {
     if (lane == 0) {
       const int t = (int)blockIdx.x + (k / spw) * (int)gridDim.x;
+      const uint32_t zb = zb0 + 8u * (uint32_t)(k & 1);
       tc::fence_async_smem();
       tc::mbar_expect_tx(zb, 2048);
-      tma_load_2d(es + kEpiF, mf, (t % g.ntn) * g.Nt + (2 * (k % spw) + par) * 32, (t / g.ntn) * 128 + q * 32, zb);
+      tma_load_2d(es + kEpiF + 2048u * (uint32_t)(k & 1), mf, (t % g.ntn) * g.Nt + (2 * (k % spw) + par) * 32,
+                  (t / g.ntn) * 128 + q * 32, zb);
     }
     ++zi;
   };
-  if (kMode == kGemmSiluBwd && nsteps > 0) z_issue(0);
+  if (kMode == kGemmSiluBwd)
+    for (int kk = 0; kk < 2 && kk < nsteps; ++kk) z_issue(kk);
   int k = 0, j = 0;
   GemmSched<kMode> sched(g);
   GemmWork tl;
@@ -416,15 +420,15 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
       float v[32];
       tc::tmem_ld32(taddr + (uint32_t)c, v);
       if (kMode == kGemmSiluBwd) {
-        if (!__all_sync(0xffffffffu, gemm_wait(zb, (uint32_t)k & 1, abort_v))) {
+        if (!__all_sync(0xffffffffu, gemm_wait(zb0 + 8u * (uint32_t)(k & 1), ((uint32_t)k >> 1) & 1, abort_v))) {
           ok = false;
           break;
         }
         ++zw;
         float z[32];
-        unstage_f16(ep + kEpiF, lane, z);
+        unstage_f16(ep + kEpiF + 2048 * (k & 1), lane, z);
         __syncwarp();  // every lane has read the box: the next one may land in its place
-        if (k + 1 < nsteps) z_issue(k + 1);
+        if (k + 2 < nsteps) z_issue(k + 2);
 #pragma unroll
         for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
         if (g.db) column_sums(g.db, v, col, nb);
@@ -439,32 +443,40 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
           v[4 * i + 3] += bb.w;
         }
       }
-      if (kMode == kGemmAtomic) {
+      if constexpr (kMode == kGemmAtomic) {
         direct_f32<true>(g.C + (size_t)row * g.ldc + col, v, nb);
-        continue;
-      }
-      float hv[32];  // the BF16 output's values
+      } else {
+        float hv[32];  // the BF16 output's values
 #pragma unroll
-      for (int i = 0; i < 32; ++i) hv[i] = kMode == kGemmSilu ? silu(v[i]) : v[i];
-      if (nb < 32) {  // narrow group: plain stores
-        if (st_f) direct_f32<false>(g.C + (size_t)row * g.ldc + col, v, nb);
-        if (st_z) direct_f16(g.Z + (size_t)row * g.ldz + col, v, nb);
-        if (st_h) direct_bf16(g, hv, row, col, nb);
-        continue;
-      }
-      if (lane == 0) bulk_wait_read0();  // the previous step's stores have read the slot
-      __syncwarp();
-      if (st_f) stage_f32(ep + kEpiF, lane, v);
-      if (st_z) stage_f16(ep + kEpiF, lane, v);
-      if (st_h) stage_bf16(ep + kEpiH, lane, hv);
-      if (st_t) stage_bf16_t(ep + kEpiT, lane, hv);
-      tc::fence_async_smem();
-      __syncwarp();
-      if (lane == 0) {
-        if (st_f || st_z) tma_store_2d(mf, col, row0, es + kEpiF);
-        if (st_h) tma_store_2d(mh, col, row0, es + kEpiH);
-        if (st_t) tma_store_2d(mt, row0, col, es + kEpiT);
-        bulk_commit();
+        for (int i = 0; i < 32; ++i) hv[i] = kMode == kGemmSilu ? silu(v[i]) : v[i];
+        if (nb < 32) {  // narrow group: plain stores
+          if (st_f) direct_f32<false>(g.C + (size_t)row * g.ldc + col, v, nb);
+          if (st_z) direct_f16(g.Z + (size_t)row * g.ldz + col, v, nb);
+          if (st_h) direct_bf16(g, hv, row, col, nb);
+          continue;
+        }
+        // the store mode alternates two FP32 boxes (its H and T slots are free): the stores of
+        // step k - 2 have read this one; the other modes' single slot: those of step k - 1
+        const uint32_t fofs = kMode == kGemmStore ? 4096u * (uint32_t)(k & 1) : 0u;
+        if (lane == 0) {
+          if (kMode == kGemmStore)
+            bulk_wait_read1();
+          else
+            bulk_wait_read0();
+        }
+        __syncwarp();
+        if (st_f) stage_f32(ep + kEpiF + fofs, lane, v);
+        if (st_z) stage_f16(ep + kEpiF, lane, v);
+        if (st_h) stage_bf16(ep + kEpiH, lane, hv);
+        if (st_t) stage_bf16_t(ep + kEpiT, lane, hv);
+        tc::fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          if (st_f || st_z) tma_store_2d(mf, col, row0, es + kEpiF + fofs);
+          if (st_h) tma_store_2d(mh, col, row0, es + kEpiH);
+          if (st_t) tma_store_2d(mt, row0, col, es + kEpiT);
+          bulk_commit();
+        }
       }
     }
     if (!ok) break;
@@ -474,7 +486,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   }
   // the Z boxes issued and not waited for have landed, the stores have completed
   for (; zw < zi; ++zw)
-    if (!tc::mbar_wait(zb, (uint32_t)zw & 1)) ok = false;
+    if (!tc::mbar_wait(zb0 + 8u * (uint32_t)(zw & 1), ((uint32_t)zw >> 1) & 1)) ok = false;
   if (lane == 0) bulk_wait_all();
   __syncwarp();
   return ok;
@@ -487,7 +499,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 const __grid_constant__ GemmOutMaps om, GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t gsm[];
   constexpr int kStages = gemm_stages<kMode>();
-  __shared__ uint64_t full[kStages], empty[kStages], accf[2], acce[2], drain, zbar[kGemmEpiWarps];
+  __shared__ uint64_t full[kStages], empty[kStages], accf[2], acce[2], drain, zbar[2 * kGemmEpiWarps];
   __shared__ uint32_t tslot;
   __shared__ int abort_flag;
   volatile int* abort_v = &abort_flag;
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       tc::mbar_init(tc::smem_u32(&accf[b]), 1);
       tc::mbar_init(tc::smem_u32(&acce[b]), kGemmEpiWarps);
     }
-    for (int w = 0; w < kGemmEpiWarps; ++w) tc::mbar_init(tc::smem_u32(&zbar[w]), 1);
+    for (int w = 0; w < 2 * kGemmEpiWarps; ++w) tc::mbar_init(tc::smem_u32(&zbar[w]), 1);
     tc::mbar_init(tc::smem_u32(&drain), 1);
     abort_flag = 0;
     tc::mbar_fence_init();
