@@ -386,6 +386,56 @@ __device__ bool policy_pass(tc::Pipe& p, PolicyShared& ps, uint8_t* smraw, int r
   return policy_layer_done(ps, ok);
 }
 
+// decim substeps of the two-role split step for one env (role 0: legs,
+// pelvis, base; role 1: waist and arms), the arithmetic of split_kernel with
+// its single call sites of the chain routines (bwd_role, fwd_role).  Kept out
+// of line so that the physics has its own register allocation: the network
+// and task state live around it is saved once per policy step instead of
+// competing with every substep for the 255 registers.  Returns the base
+// state (role 0; role 1's copy is the one it read).
+__device__ __noinline__ EnvState policy_substeps(int role, bool act, EnvState st, EnvIO io, EnvParams ep,
+                                                 StepConfig cfg, float* col, int decim) {
+  SmemScratch<kPolicyEnvs> scr{col};
+  for (int s = 0; s < decim; ++s) {
+    const bool last_sub = s == decim - 1;
+    AI acc0;
+    SV accP0;
+    EnvState su;  // role 1: the base state at the start of the substep
+    if (act) {
+      if (role == 0) {
+        fk_lower(st, io, ep, cfg, scr, last_sub);
+      } else {
+        load_base(scr, su);
+        fk_upper(su, cfg, scr);
+      }
+      bwd_role(role, role == 0 ? st : su, io, ep, cfg, scr, acc0, accP0);
+      if (role == 1) store_ai(scr, kXUp, acc0, accP0);
+    }
+    __syncthreads();
+    SV a0;
+    if (act && role == 0) {
+      AI up;
+      SV upP;
+      load_ai(scr, kXUp, up, upP);
+      ai_add(acc0, up);
+      sv_acc(accP0, upP);
+      a0 = base_solve(acc0, accP0);
+      store_sv(scr, kXA0, a0);
+    }
+    __syncthreads();
+    if (act) {
+      if (role == 1) {
+        a0 = load_sv(scr, kXA0);
+        st = su;
+      }
+      fwd_role(role, st, a0, cfg, scr);
+      if (role == 0) store_base(scr, st);
+    }
+    __syncthreads();
+  }
+  return st;
+}
+
 __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
     policy_kernel(StateArgs a, float* ctrl, int npolicy, int decim, StepConfig cfg, TaskParams tp, PolicyArgs pa,
                   TaskArgs ta, OutArgs out) {
@@ -506,46 +556,7 @@ __global__ void __launch_bounds__(2 * kPolicyEnvs, 1)
         __syncthreads();  // the substeps reuse the staging
       }
       // ---- physics: decim substeps of the split step
-      for (int s = 0; s < decim; ++s) {
-        const bool last_sub = s == decim - 1;
-        AI acc0;
-        SV accP0;
-        EnvState su;
-        if (act) {
-          if (role == 0) {
-            fk_lower(st, io, ep, cfg, scr, last_sub);
-            bwd_lower(st, io, ep, cfg, scr, acc0, accP0);
-          } else {
-            load_base(scr, su);
-            fk_upper(su, cfg, scr);
-            AI up;
-            SV upP;
-            bwd_upper(io, ep, cfg, scr, up, upP);
-            store_ai(scr, kXUp, up, upP);
-          }
-        }
-        __syncthreads();
-        SV a0;
-        if (act && role == 0) {
-          AI up;
-          SV upP;
-          load_ai(scr, kXUp, up, upP);
-          ai_add(acc0, up);
-          sv_acc(accP0, upP);
-          a0 = base_solve(acc0, accP0);
-          store_sv(scr, kXA0, a0);
-        }
-        __syncthreads();
-        if (act) {
-          if (role == 1) {
-            fwd_upper(su, load_sv(scr, kXA0), cfg, scr);
-          } else {
-            fwd_lower_and_base(st, a0, cfg, scr);
-            store_base(scr, st);
-          }
-        }
-        __syncthreads();
-      }
+      st = policy_substeps(role, act, st, io, ep, cfg, reinterpret_cast<float*>(smraw) + le, decim);
       // ---- reward, termination, timers, reset, command redraw
       if (act && role == 0) {
         float cmd[3] = {ta.cmd[e], ta.cmd[sd + e], ta.cmd[2 * sd + e]};
