@@ -122,6 +122,16 @@ int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
   return gemm_run<kGemmStore>("gemm_bf16", M, N, K, A, lda, B, ldb, g, st);
 }
 
+int g1b_gemm_bf16_acc(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                      void* stream) {
+  if (!C || ldc < N || ldc % 4 || ((uintptr_t)C & 15))
+    return fail("gemm_bf16_acc: C needs ldc >= N, ldc % 4 == 0, 16-byte alignment");
+  GemmArgs g{};
+  g.C = C;
+  g.ldc = ldc;
+  return gemm_run<kGemmAtomic>("gemm_bf16_acc", M, N, K, A, lda, B, ldb, g, static_cast<cudaStream_t>(stream));
+}
+
 int g1b_sur_linear_silu(int M, int N, int K, const void* A, int lda, const void* W, int ldw, const float* bias,
                         void* Z, int ldz, void* H, int ldh, void* Ht, int ldt, void* stream) {
   if (!H || ldh < N || ldh % 8 || ((uintptr_t)H & 15))
@@ -178,8 +188,9 @@ static int grid_1d(size_t n, int block) {
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream) {
   if (B <= 0 || D <= 0 || !Y || !T || !w || !dY || !dYt || !db || !loss) return fail("sur_loss: invalid arguments");
-  const dim3 grid((D + 31) / 32, (B + 31) / 32), block(32, 8);
-  sur_loss_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
+  if (D % 8 || kLossThreads % D) return fail("sur_loss: D must divide 256 and be a multiple of 8");
+  const int blocks = (B + kLossRows - 1) / kLossRows;
+  sur_loss_kernel<<<blocks, kLossThreads, (size_t)kLossRows * (D + 2) * 2, static_cast<cudaStream_t>(stream)>>>(
       B, D, Y, T, w, static_cast<__nv_bfloat16*>(dY), static_cast<__nv_bfloat16*>(dYt), db, loss);
   return launched("sur_loss_kernel");
 }

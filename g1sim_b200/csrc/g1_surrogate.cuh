@@ -17,56 +17,58 @@ constexpr int kSurOut = 64;  // padded outputs (35 used: qacc)
 
 // silu and silu_grad: g1_gemm.cuh (its fused epilogues use them too).
 
-// The loss kernel below works on 32 x 32 tiles (block 32 x 8): rows
-// r0..r0+31 of the batch and columns c0..c0+31, reading and writing the
-// row-major arrays along columns and the transposed copies along rows
-// through a shared-memory tile, so both sides are coalesced.
-
 // Weighted MSE over the output columns: loss += sum_r sum_c w[c] (Y - T)^2 / B;
-// dY = 2 w[c] (Y - T) / B as BF16 [B][D] and transposed [D][B]; db += sums.
-__global__ void sur_loss_kernel(int B, int D, const float* __restrict__ Y, const float* __restrict__ T,
-                                const float* __restrict__ w, __nv_bfloat16* dY, __nv_bfloat16* dYt, float* db,
-                                float* loss) {
-  __shared__ __nv_bfloat16 t[32][34];
-  __shared__ float red[2][8][33];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  const int c = c0 + threadIdx.x;
-  const float wc = c < D ? w[c] : 0.0f;
+// dY = 2 w[c] (Y - T) / B as BF16 [B][D] and transposed [D][B]; db[c] += the
+// column sums of the FP32 gradient.  One block per 128 rows, D dividing the
+// 256 threads so that each thread keeps one column: the row-major arrays are
+// read and written column-fastest (coalesced), the gradient tile is staged in
+// shared memory ([128][D + 2], conflict-free both ways) for the transposed
+// copy, and each block adds one partial sum per column and one loss term.
+constexpr int kLossRows = 128, kLossThreads = 256;
+__global__ void __launch_bounds__(kLossThreads) sur_loss_kernel(int B, int D, const float* __restrict__ Y,
+                                                                const float* __restrict__ T,
+                                                                const float* __restrict__ w, __nv_bfloat16* dY,
+                                                                __nv_bfloat16* dYt, float* db, float* loss) {
+  extern __shared__ __nv_bfloat16 tile[];  // [kLossRows][D + 2]
+  __shared__ float red[kLossThreads];
+  __shared__ float lred[kLossThreads / 32];
+  const int r0 = blockIdx.x * kLossRows;
+  const int rows = B - r0 < kLossRows ? B - r0 : kLossRows;
+  const int ld = D + 2;
+  const int c = threadIdx.x % D;
+  const float wc = w[c];
   float acc = 0.0f, l = 0.0f;
-  for (int k = threadIdx.y; k < 32; k += 8) {
-    const int r = r0 + k;
-    if (r < B && c < D) {
-      const size_t i = (size_t)r * D + c;
-      const float e = Y[i] - T[i];
-      l += wc * e * e;
-      const float g = 2.0f * wc * e / (float)B;
-      acc += g;
-      const __nv_bfloat16 gb = __float2bfloat16_rn(g);
-      dY[i] = gb;
-      t[k][threadIdx.x] = gb;
-    }
+  for (int i = threadIdx.x; i < rows * D; i += kLossThreads) {
+    const int r = i / D;
+    const size_t gi = (size_t)(r0 + r) * D + c;
+    const float e = Y[gi] - T[gi];
+    l += wc * e * e;
+    const float g = 2.0f * wc * e / (float)B;
+    acc += g;
+    const __nv_bfloat16 gb = __float2bfloat16_rn(g);
+    dY[gi] = gb;
+    tile[r * ld + c] = gb;
   }
-  red[0][threadIdx.y][threadIdx.x] = acc;
-  red[1][threadIdx.y][threadIdx.x] = l;
+  red[threadIdx.x] = acc;
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = l;
   __syncthreads();
-  for (int k = threadIdx.y; k < 32; k += 8) {
-    const int cc = c0 + k, r = r0 + threadIdx.x;
-    if (r < B && cc < D) dYt[(size_t)cc * B + r] = t[threadIdx.x][k];
+  for (int i = threadIdx.x; i < D * rows; i += kLossThreads) {
+    const int cc = i / rows, r = i - cc * rows;
+    dYt[(size_t)cc * B + r0 + r] = tile[r * ld + cc];
   }
-  if (threadIdx.y == 0) {
-    float s = 0.0f, ls = 0.0f;
-    for (int k = 0; k < 8; ++k) {
-      s += red[0][k][threadIdx.x];
-      ls += red[1][k][threadIdx.x];
-    }
-    if (c < D) atomicAdd(db + c, s);
-    // one loss atomic per block (warp sum), not one per column
-    for (int o = 16; o > 0; o >>= 1) ls += __shfl_xor_sync(0xffffffffu, ls, o);
-    if (threadIdx.x == 0) atomicAdd(loss, ls / (float)B);
+  if (threadIdx.x < D) {
+    float sum = 0.0f;
+    for (int k = threadIdx.x; k < kLossThreads; k += D) sum += red[k];
+    atomicAdd(db + threadIdx.x, sum);
+  }
+  if (threadIdx.x == 0) {
+    float ls = 0.0f;
+    for (int k = 0; k < kLossThreads / 32; ++k) ls += lred[k];
+    atomicAdd(loss, ls / (float)B);
   }
 }
 
-// Adam (Kingma & Ba 2015) with bias correction, in place on FP32 p, m, v.
 // The optimiser step of every layer in one launch: Adam on the FP32
 // weights and biases (moments m, v; bias corrections 1 - b1^t, 1 - b2^t for
 // the step count t and the learning rate read from device memory, so that a

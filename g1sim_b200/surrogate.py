@@ -51,11 +51,17 @@ def _st(dev):
     return C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
 
-def gemm(A, B, C_, bias=None, splits=1):
-    """C = A @ B^T (+ bias): A [M, K], B [N, K] BF16 row-major, C [M, N] FP32 (tcgen05 kernel)."""
+def gemm(A, B, C_, bias=None, splits=1, acc=False):
+    """C = A @ B^T (+ bias): A [M, K], B [N, K] BF16 row-major, C [M, N] FP32
+    (tcgen05 kernel).  acc: C += A @ B^T instead, K split over the SMs (no bias)."""
     M_, K = A.shape
     N = B.shape[0]
     assert B.shape[1] == K and C_.shape == (M_, N) and A.dtype == B.dtype == torch.bfloat16
+    if acc:
+        assert bias is None
+        _lib.check(_lib.lib().g1b_gemm_bf16_acc(M_, N, K, _p(A), A.stride(0), _p(B), B.stride(0), _p(C_),
+                                                C_.stride(0), _st(A.device)), "g1b_gemm_bf16_acc")
+        return
     _lib.check(_lib.lib().g1b_gemm_bf16(M_, N, K, _p(A), A.stride(0), _p(B), B.stride(0), _p(C_), C_.stride(0),
                                         _p(bias), splits, _st(A.device)), "g1b_gemm_bf16")
 
@@ -118,8 +124,16 @@ class Surrogate:
         self.vb = [torch.zeros_like(b) for b in self.b]
         self.Wb = [torch.empty(w.shape, dtype=torch.bfloat16, device=device) for w in self.W]
         self.Wt = [torch.empty(w.shape[1], w.shape[0], dtype=torch.bfloat16, device=device) for w in self.W]
-        self.gW = [torch.zeros(max(w.shape[0], 128), w.shape[1], device=device) for w in self.W]
-        self.gb = [torch.zeros_like(b) for b in self.b]
+        # every gradient and the loss in one buffer, zeroed by one launch per backward pass
+        # (the weight gradients are summed into it by split-K GEMMs)
+        shapes = [(max(w.shape[0], 128), w.shape[1]) for w in self.W] + [tuple(b.shape) for b in self.b] + [(1,)]
+        sizes = [int(np.prod(sh)) for sh in shapes]
+        self._grad = torch.zeros(sum(sizes), device=device)
+        views, off = [], 0
+        for sh, n in zip(shapes, sizes):
+            views.append(self._grad[off:off + n].view(sh))
+            off += n
+        self.gW, self.gb, self.loss_buf = views[:5], views[5:10], views[10]
         self.step_n = 0
         # Adam's step count and learning rate live on the device, so that a
         # CUDA graph of the training step replays with the current ones
@@ -156,8 +170,9 @@ class Surrogate:
                 dY=torch.zeros(B, 64, device=d),
                 dZ=torch.empty(B, 512, dtype=bf, device=d),
                 dZ2=torch.empty(B, 512, dtype=bf, device=d),
-                dZt=torch.zeros(512, B, dtype=bf, device=d),
-                loss=torch.zeros(1, device=d))
+                dZt=torch.empty(512, B, dtype=bf, device=d),
+                # the output layer's dY transposed, padded to 128 rows (rows 64-127 stay zero)
+                dYt=torch.zeros(128, B, dtype=bf, device=d))
         return self._ws[B]
 
     def features(self, qpos, qvel, anchor, ctrl, X, Xt=None, raw=None, mu=None, dmass=None):
@@ -190,30 +205,27 @@ class Surrogate:
         w = self._work(B)
         L = _lib.lib()
         st = _st(self.device)
-        for g_ in self.gb:
-            g_.zero_()
-        w["loss"].zero_()
-        dZ, dZt = w["dZ"], w["dZt"]
-        dZt[64:128].zero_()
+        self._grad.zero_()  # every parameter gradient and the loss
+        dZ, dZt, dYt = w["dZ"], w["dZt"], w["dYt"]
         wv = self.out_w if weights is None else weights
-        # dY = d loss / d Y as BF16 [B][64] (start of dZ) and [64][B] (rows of dZt)
-        _lib.check(L.g1b_sur_loss(B, 64, _p(w["Z"][5]), _p(T), _p(wv), _p(dZ), _p(dZt), _p(self.gb[4]),
-                                  _p(w["loss"]), st), "sur_loss")
+        # dY = d loss / d Y as BF16 [B][64] (start of dZ) and [64][B] (rows 0-63 of dYt)
+        _lib.check(L.g1b_sur_loss(B, 64, _p(w["Z"][5]), _p(T), _p(wv), _p(dZ), _p(dYt), _p(self.gb[4]),
+                                  _p(self.loss_buf), st), "sur_loss")
         bufs = [w["dZ"], w["dZ2"]]  # the layer's dZ and the previous layer's, alternating
         for i in range(4, -1, -1):
             Din, Dout = DIMS[i], DIMS[i + 1]
             dz = bufs[i & 1].view(-1)[:B * Dout].view(B, Dout)
             rows = max(Dout, 128)
             hin_t = w["Ht"][i] if i > 0 else Xt
-            # dW_i = dZ_i^T . H_{i-1} (split over the batch, atomically summed)
-            gemm(dZt[:rows], hin_t, self.gW[i][:rows], splits=max(1, min(64, B // 2048)))
+            # dW_i = dZ_i^T . H_{i-1} (the batch split over the SMs, summed into the zeroed gradient)
+            gemm((dYt if i == 4 else dZt)[:rows], hin_t, self.gW[i][:rows], acc=True)
             if i > 0:
                 # dZ_{i-1} = (dZ_i . W_i) * SiLU'(Z_{i-1}), its transpose and bias gradient, one kernel
                 nxt = bufs[(i - 1) & 1].view(-1)[:B * Din].view(B, Din)
                 linear_silu_bwd(dz, self.Wt[i], w["Z"][i], nxt, dHt=dZt, db=self.gb[i - 1])
             elif want_dx:
                 gemm(dz, self.Wt[0], w["dX"])
-        return w["loss"]
+        return self.loss_buf
 
     def dX(self, B):
         return self._work(B)["dX"]

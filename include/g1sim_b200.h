@@ -257,6 +257,11 @@ int g1b_adjoint_noalloc(int nenv, const g1b_config* cfg, const g1b_adjoint_probl
  *   16-byte aligned pointers. */
 int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                   const float* bias, int splits, void* stream);
+/* C[M x N] += A[M x K] . B[N x K]^T, K shared evenly by the SMs (the split
+ * form of g1b_gemm_bf16 without clearing C first): for gradients summed
+ * into buffers the caller zeroes once for several products. */
+int g1b_gemm_bf16_acc(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                      void* stream);
 /* One hidden layer of the surrogate in one GEMM with a fused epilogue
  * (same shape rules; ldh and ldz multiples of 8, ldt >= M):
  *   z = A . W^T + bias (W [N x K]); Z = z (FP16 [M][ldz], |z| clamped to
@@ -287,8 +292,9 @@ typedef struct g1b_sur_layer {
 } g1b_sur_layer;
 int g1b_sur_adam_cast(int nl, const g1b_sur_layer* layers, const int* step, const float* lr, float b1, float b2,
                       float eps, void* stream);
-/* Element-wise kernels of the surrogate: weighted MSE and its gradient,
- * BF16 weight copies. */
+/* Element-wise kernels of the surrogate: weighted MSE and its gradient
+ * (adds into db and loss; D divides 256 and is a multiple of 8), BF16
+ * weight copies. */
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream);
 int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* stream);
