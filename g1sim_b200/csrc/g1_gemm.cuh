@@ -16,17 +16,17 @@
 // finer than the BF16 activations; |z| clamped to 65000, where silu' is
 // 0 or 1) only for the SiLU derivative of the backward pass.
 //
-// One CTA per SM (320 threads) walks its work units (GemmSched): tiles of
-// 128 rows x Nt columns (Nt = min(N, 256)), blockIdx.x, + gridDim.x, ...,
-// row tiles outermost so that the column tiles of one row block run close
-// together and read its A rows from L2; in the atomic mode an equal share of
-// (tile, K chunk) pairs per CTA.  Warp roles:
+// One CTA per SM walks its work units (GemmSched): tiles of 128 rows x Nt
+// columns (Nt = min(N, 256)), blockIdx.x, + gridDim.x, ..., row tiles
+// outermost so that the column tiles of one row block run close together and
+// read its A rows from L2; in the atomic mode an equal share of (tile,
+// K chunk) pairs per CTA.  Warp roles:
 //   warp 0   (one lane) TMA producer: for every 64-wide K chunk of a tile,
 //            waits until the MMAs have released the stage, then copies the
 //            A chunk (128 x 64) and the B chunk (Nt x 64) with
 //            cp.async.bulk.tensor (tensor maps over this GPU's memory, no
-//            multicast) into a 3-stage ring (4 in the atomic mode); the copies complete on
-//            the stage's `full` mbarrier (transaction bytes);
+//            multicast) into the ring (EpiCfg::kStages deep); the copies
+//            complete on the stage's `full` mbarrier (transaction bytes);
 //   warp 1   (one lane) MMA issuer: per chunk waits on `full`, issues four
 //            tcgen05.mma (M 128, N Nt, K 16) into one of two tensor-memory
 //            accumulators and commits them to the stage's `empty` barrier;
@@ -34,18 +34,19 @@
 //            barrier, and before a tile waits until the epilogue has
 //            drained that accumulator (its `empty` barrier, one arrival per
 //            epilogue warp);
-//   warps 2-9 epilogue, two per TMEM lane quarter (warp w may access lanes
-//            32 (w % 4) .. + 31, i.e. 32 rows of the tile), one taking the
-//            even and one the odd 32-column groups: tcgen05.ld, the mode's
-//            arithmetic, then the 32 x 32 results go to the warp's staging
-//            buffer in shared memory in the layout of the output's tensor
-//            map and one lane stores them with cp.async.bulk.tensor (whole
-//            lines to global memory instead of one row per lane).  Two
-//            warps per SM sub-partition hide each other's latencies, and the
-//            MMAs of the next tile run on the other accumulator meanwhile.
-//            The backward mode's pre-activation Z comes in the same way, one
-//            step ahead (TMA load into the staging buffer, one mbarrier per
-//            warp).  The bias of the warp's columns is staged once per tile.
+//   warps 2.. epilogue (EpiCfg::kWarps: 8 or 12, i.e. 2 or 3 per TMEM lane
+//            quarter; warp w may access lanes 32 (w % 4) .. + 31, i.e. 32
+//            rows of the tile), sharing the tile's 32-column groups:
+//            tcgen05.ld, the mode's arithmetic, then the 32 x 32 results go
+//            to the warp's staging buffer in shared memory in the layout of
+//            the output's tensor map and one lane stores them with
+//            cp.async.bulk.tensor (whole lines to global memory instead of
+//            one row per lane).  Several warps per SM sub-partition hide
+//            each other's latencies, and the MMAs of the next tile run on
+//            the other accumulator meanwhile.  The backward mode's
+//            pre-activation Z comes in the same way, ahead of its step (TMA
+//            load into the staging buffer, per-warp mbarriers).  The bias of
+//            the warp's columns is staged once per tile.
 // Operand tiles land in the UMMA K-major 128-byte-swizzle layout (each row's
 // 64 values one 128-byte line, eight lines a 1024-byte atom, 16-byte piece j
 // of row r at piece j ^ (r % 8)), the tensor map's SWIZZLE_128B.  Staging
@@ -70,27 +71,35 @@
 constexpr int kGemmKC = 64;  // K columns per chunk (one 128-byte swizzle line)
 constexpr int kGemmMaxN = 256;
 constexpr int kGemmMaxStages = 4;
-constexpr int kGemmEpiWarps = 8;  // two per TMEM lane quarter
-constexpr int kGemmThreads = 64 + 32 * kGemmEpiWarps;
 constexpr uint32_t kGemmABytes = 128 * kGemmKC * 2;        // 16 KB
 constexpr uint32_t kGemmBBytes = kGemmMaxN * kGemmKC * 2;  // 32 KB
 constexpr uint32_t kGemmStageBytes = kGemmABytes + kGemmBBytes;
 constexpr uint32_t kGemmAccCols = 256;  // one accumulator; two of them fill the 512 TMEM columns
-// Per epilogue warp one staging slot of: FP32 box 4 KB (output C) or FP16
-// box 2 KB (output Z, or the Z input), BF16 box 2 KB (H), transposed BF16
-// box 2 KB (Ht); and the bias of its columns of the tile (128 floats).
-constexpr uint32_t kEpiF = 0, kEpiH = 4096, kEpiT = 6144, kEpiWarpBytes = 8192, kEpiBiasBytes = 512;
-// Operand ring depth: three stages next to the epilogue staging; four in the
-// atomic mode, whose epilogue adds straight into C and stages nothing (its
-// operands both stream from DRAM, so it needs the deeper ring most).
+constexpr uint32_t kEpiBiasBytes = 512;  // per epilogue warp: the bias of its columns of a tile
+constexpr int kGemmMaxEpiWarps = 12;
+
+// Per mode: operand ring depth, epilogue warps (a multiple of four: 2 or 3
+// per TMEM lane quarter, so 2 or 3 per SM sub-partition to hide each other's
+// latencies) and each warp's staging layout (byte offsets of its FP32 / FP16
+// box F, BF16 box H and transposed BF16 box T; FBoxes boxes alternate in F).
+//   store    3 stages, 8 warps: two 4 KB FP32 boxes
+//   atomic   4 stages (its epilogue adds straight into C and stages nothing,
+//            and its operands both stream from DRAM), 8 warps
+//   silu     3 stages, 12 warps: FP16 Z 2 KB, H 2 KB, T 2 KB
+//   silu_bwd 3 stages, 12 warps: one FP16 Z input box 2 KB, H 2 KB, T 2 KB
 template <int kMode>
-__host__ __device__ constexpr int gemm_stages() { return kMode == 1 ? 4 : 3; }
-template <int kMode>
-__host__ __device__ constexpr uint32_t gemm_epi_bytes() { return kMode == 1 ? 0u : kGemmEpiWarps * kEpiWarpBytes; }
+struct EpiCfg {
+  static constexpr int kStages = kMode == 1 ? 4 : 3;
+  static constexpr int kWarps = kMode >= 2 ? 12 : 8;
+  static constexpr uint32_t kF = 0, kH = 2048, kT = 4096;
+  static constexpr uint32_t kBytes = kMode == 1 ? 0u : (kMode == 0 ? 8192u : 6144u);
+  static constexpr int kFBoxes = kMode == 0 ? 2 : 1;
+  static constexpr int kThreads = 64 + 32 * kWarps;
+};
 template <int kMode>
 __host__ __device__ constexpr size_t gemm_smem() {
-  return gemm_stages<kMode>() * (size_t)kGemmStageBytes + gemm_epi_bytes<kMode>() +
-         kGemmEpiWarps * (size_t)kEpiBiasBytes + 1024;
+  return EpiCfg<kMode>::kStages * (size_t)kGemmStageBytes +
+         EpiCfg<kMode>::kWarps * (size_t)(EpiCfg<kMode>::kBytes + kEpiBiasBytes) + 1024;
 }
 
 enum GemmMode : int { kGemmStore = 0, kGemmAtomic = 1, kGemmSilu = 2, kGemmSiluBwd = 3 };
@@ -347,9 +356,9 @@ __device__ __forceinline__ void column_sums(float* db, const float (&v)[32], int
   if (lane < nb) atomicAdd(db + col + lane, w[0]);
 }
 
-// The epilogue role (warps 2 .. 2 + kGemmEpiWarps - 1).  Warp w owns TMEM
-// lane quarter w % 4 (rows 32 (w % 4) .. + 31 of the tile) and, of the tile's
-// 32-column groups, the even ones (w < 6) or the odd ones (w >= 6).  mf / mh
+// The epilogue role (warps 2 .. 2 + kWarps - 1).  Warp w owns TMEM lane
+// quarter w % 4 (rows 32 (w % 4) .. + 31 of the tile) and, of the tile's
+// 32-column groups, those g with g % P == (w - 2) / 4 (P = kWarps / 4).  mf / mh
 // / mt: the output maps (kernel parameters, so their generic addresses stay
 // valid for TMA).
 template <int kMode>
@@ -360,18 +369,21 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = warp & 3;   // TMEM lane quarter = the warp's 32 rows of the tile
   const int ew = warp - 2;  // staging area and mbarrier of this warp
-  const int par = ew >> 2;  // the warp's column groups: par, par + 2, ...
-  uint8_t* const ep = ep0 + (size_t)ew * kEpiWarpBytes;
-  const uint32_t es = ebase0 + (uint32_t)ew * kEpiWarpBytes;
-  float* const sbias = reinterpret_cast<float*>(ep0 + gemm_epi_bytes<kMode>() + ew * kEpiBiasBytes);
-  const uint32_t zb0 = tc::smem_u32(&zbar[2 * ew]);  // Z box k in slot k % 2: barrier zb0 + 8 (k % 2)
+  using E = EpiCfg<kMode>;
+  constexpr int P = E::kWarps / 4;                  // warps per lane quarter
+  constexpr int ZB = E::kWarps == 12 ? 1 : 2;      // backward: Z boxes in flight (the staging holds them)
+  const int par = ew >> 2;  // the warp's column groups: par, par + P, ...
+  uint8_t* const ep = ep0 + (size_t)ew * E::kBytes;
+  const uint32_t es = ebase0 + (uint32_t)ew * E::kBytes;
+  float* const sbias = reinterpret_cast<float*>(ep0 + (size_t)E::kWarps * E::kBytes + ew * kEpiBiasBytes);
+  const uint32_t zb0 = tc::smem_u32(&zbar[2 * ew]);  // Z box k: slot k % ZB, barrier zb0 + 8 (k % ZB)
   const bool st_f = kMode == kGemmStore;                      // FP32 C
   const bool st_z = kMode == kGemmSilu && g.Z != nullptr;      // FP16 Z
   const bool st_h = kMode == kGemmSilu || kMode == kGemmSiluBwd;
   const bool st_t = st_h && g.Ht != nullptr;
   const bool has_bias = g.bias != nullptr && kMode != kGemmSiluBwd;
   const int ngroups = (g.Nt + 31) / 32;
-  const int spw = (ngroups - par + 1) / 2;  // this warp's groups per tile
+  const int spw = (ngroups - par + P - 1) / P;  // this warp's groups per tile
   // steps of the backward mode's Z prefetch (whole tiles blockIdx.x, + gridDim.x, ...)
   const int my_tiles = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int nsteps = my_tiles * spw;
@@ -381,16 +393,16 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   auto z_issue = [&](int k) {
     if (lane == 0) {
       const int t = (int)blockIdx.x + (k / spw) * (int)gridDim.x;
-      const uint32_t zb = zb0 + 8u * (uint32_t)(k & 1);
+      const uint32_t zb = zb0 + 8u * (uint32_t)(k % ZB);
       tc::fence_async_smem();
       tc::mbar_expect_tx(zb, 2048);
-      tma_load_2d(es + kEpiF + 2048u * (uint32_t)(k & 1), mf, (t % g.ntn) * g.Nt + (2 * (k % spw) + par) * 32,
+      tma_load_2d(es + E::kF + 2048u * (uint32_t)(k % ZB), mf, (t % g.ntn) * g.Nt + (P * (k % spw) + par) * 32,
                   (t / g.ntn) * 128 + q * 32, zb);
     }
     ++zi;
   };
   if (kMode == kGemmSiluBwd)
-    for (int kk = 0; kk < 2 && kk < nsteps; ++kk) z_issue(kk);
+    for (int kk = 0; kk < ZB && kk < nsteps; ++kk) z_issue(kk);
   int k = 0, j = 0;
   GemmSched<kMode> sched(g);
   GemmWork tl;
@@ -400,7 +412,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
     if (add_bias) {  // this warp's bias values of the tile
       __syncwarp();
       for (int s = 0; s < spw; ++s) {
-        const int c = (2 * s + par) * 32 + lane;
+        const int c = (P * s + par) * 32 + lane;
         sbias[s * 32 + lane] = c < g.Nt ? __ldg(g.bias + tl.n * g.Nt + c) : 0.0f;  // exactly N floats
       }
       __syncwarp();
@@ -414,21 +426,21 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
     const int row0 = tl.m * 128 + q * 32, row = row0 + lane;
     const uint32_t taddr = tmem + (uint32_t)b * kGemmAccCols + ((uint32_t)(q * 32) << 16);
     for (int s = 0; s < spw; ++s, ++k) {
-      const int c = (2 * s + par) * 32;
+      const int c = (P * s + par) * 32;
       const int nb = g.Nt - c < 32 ? g.Nt - c : 32;
       const int col = tl.n * g.Nt + c;
       float v[32];
       tc::tmem_ld32(taddr + (uint32_t)c, v);
       if (kMode == kGemmSiluBwd) {
-        if (!__all_sync(0xffffffffu, gemm_wait(zb0 + 8u * (uint32_t)(k & 1), ((uint32_t)k >> 1) & 1, abort_v))) {
+        if (!__all_sync(0xffffffffu, gemm_wait(zb0 + 8u * (uint32_t)(k % ZB), (uint32_t)(k / ZB) & 1, abort_v))) {
           ok = false;
           break;
         }
         ++zw;
         float z[32];
-        unstage_f16(ep + kEpiF + 2048 * (k & 1), lane, z);
+        unstage_f16(ep + E::kF + 2048 * (k % ZB), lane, z);
         __syncwarp();  // every lane has read the box: the next one may land in its place
-        if (k + 2 < nsteps) z_issue(k + 2);
+        if (k + ZB < nsteps) z_issue(k + ZB);
 #pragma unroll
         for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
         if (g.db) column_sums(g.db, v, col, nb);
@@ -457,7 +469,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
         }
         // the store mode alternates two FP32 boxes (its H and T slots are free): the stores of
         // step k - 2 have read this one; the other modes' single slot: those of step k - 1
-        const uint32_t fofs = kMode == kGemmStore ? 4096u * (uint32_t)(k & 1) : 0u;
+        const uint32_t fofs = 4096u * (uint32_t)(k % E::kFBoxes);
         if (lane == 0) {
           if (kMode == kGemmStore)
             bulk_wait_read1();
@@ -465,16 +477,16 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
             bulk_wait_read0();
         }
         __syncwarp();
-        if (st_f) stage_f32(ep + kEpiF + fofs, lane, v);
-        if (st_z) stage_f16(ep + kEpiF, lane, v);
-        if (st_h) stage_bf16(ep + kEpiH, lane, hv);
-        if (st_t) stage_bf16_t(ep + kEpiT, lane, hv);
+        if (st_f) stage_f32(ep + E::kF + fofs, lane, v);
+        if (st_z) stage_f16(ep + E::kF, lane, v);
+        if (st_h) stage_bf16(ep + E::kH, lane, hv);
+        if (st_t) stage_bf16_t(ep + E::kT, lane, hv);
         tc::fence_async_smem();
         __syncwarp();
         if (lane == 0) {
-          if (st_f || st_z) tma_store_2d(mf, col, row0, es + kEpiF + fofs);
-          if (st_h) tma_store_2d(mh, col, row0, es + kEpiH);
-          if (st_t) tma_store_2d(mt, row0, col, es + kEpiT);
+          if (st_f || st_z) tma_store_2d(mf, col, row0, es + E::kF + fofs);
+          if (st_h) tma_store_2d(mh, col, row0, es + E::kH);
+          if (st_t) tma_store_2d(mt, row0, col, es + E::kT);
           bulk_commit();
         }
       }
@@ -486,7 +498,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   }
   // the Z boxes issued and not waited for have landed, the stores have completed
   for (; zw < zi; ++zw)
-    if (!tc::mbar_wait(zb0 + 8u * (uint32_t)(zw & 1), ((uint32_t)zw >> 1) & 1)) ok = false;
+    if (!tc::mbar_wait(zb0 + 8u * (uint32_t)(zw % ZB), (uint32_t)(zw / ZB) & 1)) ok = false;
   if (lane == 0) bulk_wait_all();
   __syncwarp();
   return ok;
@@ -494,12 +506,12 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
 
 // ---------------------------------------------------------------- kernel
 template <int kMode>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ GemmOutMaps om, GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t gsm[];
-  constexpr int kStages = gemm_stages<kMode>();
-  __shared__ uint64_t full[kStages], empty[kStages], accf[2], acce[2], drain, zbar[2 * kGemmEpiWarps];
+  constexpr int kStages = EpiCfg<kMode>::kStages;
+  __shared__ uint64_t full[kStages], empty[kStages], accf[2], acce[2], drain, zbar[2 * kGemmMaxEpiWarps];
   __shared__ uint32_t tslot;
   __shared__ int abort_flag;
   volatile int* abort_v = &abort_flag;
@@ -516,9 +528,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(tc::smem_u32(&accf[b]), 1);
-      tc::mbar_init(tc::smem_u32(&acce[b]), kGemmEpiWarps);
+      tc::mbar_init(tc::smem_u32(&acce[b]), EpiCfg<kMode>::kWarps);
     }
-    for (int w = 0; w < 2 * kGemmEpiWarps; ++w) tc::mbar_init(tc::smem_u32(&zbar[w]), 1);
+    for (int w = 0; w < 2 * EpiCfg<kMode>::kWarps; ++w) tc::mbar_init(tc::smem_u32(&zbar[w]), 1);
     tc::mbar_init(tc::smem_u32(&drain), 1);
     abort_flag = 0;
     tc::mbar_fence_init();

@@ -101,7 +101,7 @@ static int gemm_run(const char* what, int M, int N, int K, const void* A, int ld
   const int grid = units < sms ? (int)units : sms;
   if ((e = prepare<20, kMode>(gemm_kernel<kMode>, gemm_smem<kMode>())) != cudaSuccess)
     return cuda_fail(e, "gemm: attributes");
-  gemm_kernel<kMode><<<grid, kGemmThreads, gemm_smem<kMode>(), st>>>(ma, mb, om, g);
+  gemm_kernel<kMode><<<grid, EpiCfg<kMode>::kThreads, gemm_smem<kMode>(), st>>>(ma, mb, om, g);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : cuda_fail(e, "gemm_kernel");
 }
