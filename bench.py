@@ -477,9 +477,10 @@ def adjoint_bench(device, stream, steps, warmup, world, n=ADJ_ENVS, horizon=ADJ_
     for _ in range(max(1, warmup)):
         one()
     times, r = [], None
-    for _ in range(max(1, steps)):
-        t, r = one()
-        times.append(t)
+    with ClockSampler(device.index if device.index is not None else 0) as clk:
+        for _ in range(max(3, steps)):
+            t, r = one()
+            times.append(t)
     ms = max_over_ranks(statistics.mean(times), world, device)
     # the plain step on the same envs for the same horizon (H substeps, one launch), for the cost ratio
     from g1sim_b200 import _lib
@@ -497,7 +498,7 @@ def adjoint_bench(device, stream, steps, warmup, world, n=ADJ_ENVS, horizon=ADJ_
     stream.synchronize()
     plain_ms = e0.elapsed_time(e1) / 5
     return {"value": float(n) * H * world / (ms * 1e-3), "unit": "env-steps/s (horizon steps differentiated)",
-            "ms_per_call": ms,
+            "ms_per_call": ms, "ms_per_call_each": times, "clocks": clk.summary(),
             "plain_step_same_envs": {"ms": plain_ms, "value": float(n) * H / (plain_ms * 1e-3),
                                      "note": f"g1b_step, {n} envs x {H} substeps in one launch"},
             "cost_vs_plain_same_envs": ms / plain_ms,
