@@ -24,8 +24,8 @@
 //   warp 0   (one lane) TMA producer: for every 64-wide K chunk of a tile,
 //            waits until the MMAs have released the stage, then copies the
 //            A chunk (128 x 64) and the B chunk (Nt x 64) with
-//            cp.async.bulk.tensor (tensor maps over this GPU's memory, no
-//            multicast) into the ring (EpiCfg::kStages deep); the copies
+//            cp.async.bulk.tensor (tensor maps over this GPU's memory, each
+//            copy into this CTA only) into the ring (EpiCfg::kStages deep); the copies
 //            complete on the stage's `full` mbarrier (transaction bytes);
 //   warp 1   (one lane) MMA issuer: per chunk waits on `full`, issues four
 //            tcgen05.mma (M 128, N Nt, K 16) into one of two tensor-memory

@@ -86,7 +86,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (globaltimer() - t0 > kWaitNs) return false;
   return true;
 }
-// Bulk global -> shared copy completing on an mbarrier (no multicast).
+// Bulk global -> shared copy into this CTA only, completing on an mbarrier.
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
