@@ -8,7 +8,9 @@
     points, to 3e-3 relative in 2-norm (the two sides may round a hidden
     activation to neighbouring BF16 values when their sums differ in the
     last bits);
-  * Adam against its published update rule on the CPU;
+  * Adam against its published update rule on the CPU, over three steps of
+    the fused optimiser launch (device step count and learning rate);
+  * training steps replayed from the captured CUDA graph equal eager ones;
   * training on transitions of the randomised workload lowers the loss;
   * the fallback rollout with bound 0 is the exact step, bit for bit, and
     with the trained network stays finite;
@@ -231,6 +233,60 @@ def test_adam_matches_update_rule():
     # BF16 copies refreshed
     assert torch.equal(sur.Wb[0], sur.W[0].to(torch.bfloat16))
     assert torch.equal(sur.Wt[0], sur.W[0].T.contiguous().to(torch.bfloat16))
+
+
+def test_adam_bias_correction_over_steps():
+    """Three steps of the fused optimiser launch (step count and learning
+    rate in device memory) against Adam's update rule with t = 1, 2, 3."""
+    sur = S.Surrogate(DEV, seed=4)
+    w = sur.W[1].clone().double()
+    m = torch.zeros_like(w)
+    v = torch.zeros_like(w)
+    g = torch.Generator(device=DEV).manual_seed(5)
+    for t, lr in ((1, 1e-2), (2, 5e-3), (3, 2e-3)):
+        gw = torch.randn(sur.W[1].shape, device=DEV, generator=g)
+        sur.gW[1][:gw.shape[0]].copy_(gw)
+        sur.adam(lr=lr)
+        torch.cuda.synchronize()
+        m = 0.9 * m + 0.1 * gw.double()
+        v = 0.999 * v + 0.001 * gw.double() ** 2
+        w = w - lr * (m / (1 - 0.9 ** t)) / (torch.sqrt(v / (1 - 0.999 ** t)) + 1e-8)
+        assert torch.allclose(sur.W[1].double(), w, rtol=1e-5, atol=1e-6), t
+    assert int(sur.opt_step.item()) == 3 and sur.step_n == 3
+    assert torch.equal(sur.Wt[1], sur.W[1].T.contiguous().to(torch.bfloat16))
+
+
+def test_train_graph_replays_the_eager_step():
+    """Training steps replayed from the captured CUDA graph give the weights
+    of the same steps launched eagerly, up to the order of the atomic sums:
+    Adam's normalised update turns that noise (and the BF16 activations it
+    can flip) into weight differences of up to a few 1e-5 where a gradient
+    is small, and an entry whose gradient changes sign can move by up to
+    2 lr.  So every tensor agrees to 1e-3 relative in norm (measured ~1e-5)
+    and no entry differs by more than twice the summed learning rates; a
+    replay with a stale learning rate would be off by 2e-4 - 6e-4 per step
+    almost everywhere, a few percent of the weights' norm."""
+    B = 4096
+    g = torch.Generator(device=DEV).manual_seed(6)
+    X = bf(torch.randn(B, S.NIN, device=DEV, generator=g))
+    X[:, S.NFEAT:] = 0
+    Xt = X.T.contiguous()
+    T = torch.randn(B, 64, device=DEV, generator=g)
+    a, b = S.Surrogate(DEV, seed=7), S.Surrogate(DEV, seed=7)
+    lrs = [1e-3, 8e-4, 6e-4, 4e-4]
+    for lr in lrs:
+        la = float(a.train_step(X, Xt, T, lr=lr).item())
+    tg = b.capture_train_step(X, Xt, T, lrs[0])  # runs the first step eagerly
+    for lr in lrs[1:]:
+        lb = float(tg.step(lr).item())
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    assert a.step_n == b.step_n == len(lrs) and int(b.opt_step.item()) == len(lrs)
+    assert abs(la - lb) <= 1e-5 * abs(la)
+    for wa, wb in zip(a.W + a.b, b.W + b.b):
+        d = (wa - wb).abs()
+        assert d.norm().item() <= 1e-3 * wa.norm().item()
+        assert d.max().item() <= 2 * sum(lrs)
 
 
 @pytest.fixture(scope="module")
