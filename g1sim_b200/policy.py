@@ -329,7 +329,9 @@ def ppo_update(ac, optimizer, buf, returns, advs, epochs=5, minibatches=4, clip=
     b_values = buf.values.reshape(-1)
     n = b_obs.shape[0]
     mb = n // minibatches
-    kl_sum, count = 0.0, 0
+    # the KL of each minibatch is summed on the device and read once at the end
+    # (the reference reads it per minibatch, train.py:402-403; one sync instead of 20)
+    kl_sum, count = torch.zeros((), dtype=torch.float64, device=b_obs.device), 0
     for ep in range(epochs):
         idx = perms[ep] if perms is not None else torch.randperm(n, device=b_obs.device, generator=generator)
         for s in range(0, n, mb):
@@ -345,6 +347,6 @@ def ppo_update(ac, optimizer, buf, returns, advs, epochs=5, minibatches=4, clip=
             nn.utils.clip_grad_norm_(ac.parameters(), max_grad_norm)
             optimizer.step()
             with torch.no_grad():
-                kl_sum += (b_logp[j] - new_logp).mean().item()
+                kl_sum += (b_logp[j] - new_logp).mean()
                 count += 1
-    return kl_sum / max(count, 1)
+    return float(kl_sum.item()) / max(count, 1)
