@@ -37,6 +37,12 @@ sys.path.insert(0, ROOT)
 # algorithm's counted add/sub/mul with its per-step recomputation of constant
 # tree rotations, spatial inertias and hinge S vectors removed.
 FLOPS_PER_ENV_STEP = 36600.0
+# The same count with the reference's per-step recomputation kept (its code as
+# written, 8 contacts active), reported alongside.
+FLOPS_PER_ENV_STEP_AS_WRITTEN = 40544.0
+# FP32 flops executed per env-substep by split_kernel (ncu: FFMA x 2 + FADD +
+# FMUL thread instructions of one 16,384-env launch over its env-substeps).
+FLOPS_EXECUTED_PER_ENV_STEP = 31385.0
 # Algorithmic bytes per env per launch: SoA state in (qpos 36, qvel 35,
 # anchor 16, ctrl 29, mu, dmass) and out (qpos, qvel, anchor, ctrl), float32.
 BYTES_PER_ENV_LAUNCH = 4.0 * ((36 + 35 + 16 + 29 + 2) + (36 + 35 + 16 + 29))
@@ -903,7 +909,11 @@ def ours(args, world, rank, local):
                          "traffic_source": "ncu DRAM bytes of one split_kernel launch at 16,384 envs, scaled by envs",
                          "algorithmic_bytes": BYTES_PER_ENV_LAUNCH * n,
                          "peak_source": "measured FFMA microbenchmark (g1b_ffma_peak), this run",
-                         "flops_per_env_step": FLOPS_PER_ENV_STEP, "kernel": kernel_name,
+                         "flops_per_env_step": FLOPS_PER_ENV_STEP,
+                         "achieved_as_written": achieved_tf * FLOPS_PER_ENV_STEP_AS_WRITTEN / FLOPS_PER_ENV_STEP,
+                         "flops_per_env_step_as_written": FLOPS_PER_ENV_STEP_AS_WRITTEN,
+                         "achieved_executed": achieved_tf * FLOPS_EXECUTED_PER_ENV_STEP / FLOPS_PER_ENV_STEP,
+                         "flops_per_env_step_executed": FLOPS_EXECUTED_PER_ENV_STEP, "kernel": kernel_name,
                          "kernel_ms": launch_ms, "hbm_gbs": hbm_gbs},
             "e2e": {"value": e2e_value, "unit": "env-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
