@@ -1,5 +1,5 @@
-// g1_policy.cuh -- the policy-fused rollout kernel (included by g1_kernels.cu
-// inside namespace g1b, after the split step kernel).
+// g1_policy.cuh -- the policy-fused rollout kernel (included by g1_policy.cu
+// inside namespace g1b, after g1_env.cuh and g1_mlp.cuh).
 //
 // One CTA owns 128 envs for the whole call (two threads per env, the split
 // step's lower/upper-body roles).  Each policy step runs, inside the CTA:

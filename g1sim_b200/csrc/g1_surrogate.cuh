@@ -1,5 +1,5 @@
 // g1_surrogate.cuh -- kernels of the learned one-step dynamics surrogate
-// (included by g1_kernels.cu inside namespace g1b, after g1_gemm.cuh).
+// (included by g1_surrogate.cu inside namespace g1b, after g1_gemm.cuh).
 //
 // The surrogate is an MLP 192 -> 512 -> 512 -> 512 -> 512 -> 64 with SiLU on
 // the hidden layers, over a normalised feature vector of the state and the
