@@ -541,6 +541,13 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
   tc::tc_fence_after();
   const uint32_t tmem = tslot;
   bool ok = true;
+  // Launched as a programmatic dependent of the previous kernel on the stream:
+  // the setup above may overlap that kernel's last CTAs; nothing below reads
+  // or writes global memory before it has completed and its writes are
+  // visible.  Our own dependents may be scheduled from now on (they wait the
+  // same way).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (warp == 0) {
     if (lane == 0) {  // ---- TMA producer

@@ -101,7 +101,19 @@ static int gemm_run(const char* what, int M, int N, int K, const void* A, int ld
   const int grid = units < sms ? (int)units : sms;
   if ((e = prepare<20, kMode>(gemm_kernel<kMode>, gemm_smem<kMode>())) != cudaSuccess)
     return cuda_fail(e, "gemm: attributes");
-  gemm_kernel<kMode><<<grid, EpiCfg<kMode>::kThreads, gemm_smem<kMode>(), st>>>(ma, mb, om, g);
+  // programmatic dependent launch: this kernel's setup may overlap the previous kernel's tail
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = dim3(grid);
+  lc.blockDim = dim3(EpiCfg<kMode>::kThreads);
+  lc.dynamicSmemBytes = gemm_smem<kMode>();
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  e = cudaLaunchKernelEx(&lc, gemm_kernel<kMode>, ma, mb, om, g);
+  if (e != cudaSuccess) return cuda_fail(e, "gemm_kernel");
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : cuda_fail(e, "gemm_kernel");
 }
