@@ -593,7 +593,9 @@ def surrogate_bench(device, train_steps, world):
     mu, dm = (torch.tensor(w[k], dtype=torch.float32, device=device) for k in ("mu", "dmass"))
     from g1sim_b200 import g1sim as G
     G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 20, DECIM, config=_cfg(), seed=7, mu=mu, dmass=dm)
+    st_loose = {k: v.clone() for k, v in st.items()}
     frac, err = S.rollout_with_fallback(sur, st, 50, bound=1e-3, mu=mu, dmass=dm)
+    frac_loose, _ = S.rollout_with_fallback(sur, st_loose, 50, bound=1e-1, mu=mu, dmass=dm)
     ref = refinement_bench(sur, device)
     peak, sustained = measured_bf16_peak(), measured_bf16_peak("bf16_tflops_sustained")
     return {"train_step_ms": step_ms, "train_step_eager_ms": timed["eager"], "train_tflops": train_tflops,
@@ -605,7 +607,8 @@ def surrogate_bench(device, train_steps, world):
             "transitions": int(X.shape[0]), "generation_s": gen_s, "train_steps": train_steps,
             "loss_start": l0, "loss_end": l1,
             "fallback_rollout": {"envs": SUR_ENVS, "steps": 50, "bound": 1e-3, "start": "after 20 policy steps",
-                                 "fraction_surrogate": frac, "one_step_error": err},
+                                 "fraction_surrogate": frac, "one_step_error": err,
+                                 "second_bound": {"bound": 1e-1, "fraction_surrogate": frac_loose}},
             "refinement": ref,
             "gemm_status": S.gemm_status()}
 
