@@ -93,8 +93,11 @@ struct EpiCfg {
   static constexpr int kWarps = kMode >= 2 ? 12 : 8;
   static constexpr uint32_t kF = 0, kH = 2048, kT = 4096;
   static constexpr uint32_t kBytes = kMode == 1 ? 0u : (kMode == 0 ? 8192u : 6144u);
-  static constexpr int kFBoxes = kMode == 0 ? 2 : 1;
+  static constexpr int kFBoxes = kMode == 0 ? 2 : 1;  // store mode: FP32 boxes alternating in F
+  static constexpr int kZBoxes = 1;                    // backward: FP16 Z boxes in flight in F
   static constexpr int kThreads = 64 + 32 * kWarps;
+  static_assert(kMode != 3 || kF + 2048u * kZBoxes <= kH, "the Z boxes must fit below H");
+  static_assert(kMode != 0 || kFBoxes * 4096u <= kBytes, "the FP32 boxes must fit the staging");
 };
 template <int kMode>
 __host__ __device__ constexpr size_t gemm_smem() {
@@ -371,7 +374,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   const int ew = warp - 2;  // staging area and mbarrier of this warp
   using E = EpiCfg<kMode>;
   constexpr int P = E::kWarps / 4;                  // warps per lane quarter
-  constexpr int ZB = E::kWarps == 12 ? 1 : 2;      // backward: Z boxes in flight (the staging holds them)
+  constexpr int ZB = E::kZBoxes;                   // backward: Z boxes in flight
   const int par = ew >> 2;  // the warp's column groups: par, par + P, ...
   uint8_t* const ep = ep0 + (size_t)ew * E::kBytes;
   const uint32_t es = ebase0 + (uint32_t)ew * E::kBytes;
@@ -388,7 +391,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
   const int my_tiles = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int nsteps = my_tiles * spw;
   bool ok = true;
-  int zi = 0, zw = 0;  // backward: Z boxes issued, waited for (two in flight)
+  int zi = 0, zw = 0;  // backward: Z boxes issued, waited for
   // backward: TMA load of the Z box of step k (this warp's rows and group)
   auto z_issue = [&](int k) {
     if (lane == 0) {
