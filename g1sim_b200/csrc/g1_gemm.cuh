@@ -194,19 +194,35 @@ struct GemmWork {
   int m, n, k0, nk;
 };
 // The CTA's sequence of work units (the producer, the MMA lane and the
-// epilogue walk the same one).  Atomic mode (stream-K): the CTA's contiguous
-// share [b T / G, (b + 1) T / G) of the T = tiles x K-chunks (tile, chunk)
-// pairs, cut at tile boundaries, so every SM gets the same number of chunks
-// whatever the tile count; partial tiles meet in C through the atomic adds.
-// Other modes: whole tiles blockIdx.x, + gridDim.x, ...
+// epilogue walk the same one).  Atomic mode (split K): with fewer tiles than
+// CTAs, cpt = G / tiles CTAs per tile, each a contiguous share of the tile's
+// K chunks (the same shares for every tile); otherwise (stream-K) the CTA's
+// contiguous share [b T / G, (b + 1) T / G) of the T = tiles x K-chunks
+// (tile, chunk) pairs, cut at tile boundaries.  Either way every SM gets
+// (nearly) the same number of chunks whatever the tile count; partial tiles
+// meet in C through the atomic adds.  Other modes: whole tiles blockIdx.x,
+// + gridDim.x, ...
 template <int kMode>
 struct GemmSched {
   int pos, end;
   __device__ explicit GemmSched(const GemmArgs& g) {
     if (kMode == kGemmAtomic) {
-      const long long T = (long long)g.ntm * g.ntn * g.nk;
-      pos = (int)(T * blockIdx.x / gridDim.x);
-      end = (int)(T * (blockIdx.x + 1) / gridDim.x);
+      const int ntiles = g.ntm * g.ntn, G = (int)gridDim.x;
+      if (ntiles < G) {
+        // every tile gets cpt CTAs and the same split of its K chunks, so the
+        // CTAs that read one operand chunk for different tiles (the column
+        // tiles of a row block, the row tiles of a column block) fetch it at
+        // the same time and all but the first find it in L2
+        const int cpt = G / ntiles, b = (int)blockIdx.x;
+        const int t = b / cpt, s = b - t * cpt;
+        const int k0 = (int)((long long)g.nk * s / cpt), k1 = (int)((long long)g.nk * (s + 1) / cpt);
+        pos = t * g.nk + k0;
+        end = b < cpt * ntiles ? t * g.nk + k1 : pos;  // the G - cpt * ntiles spare CTAs idle
+      } else {
+        const long long T = (long long)ntiles * g.nk;
+        pos = (int)(T * blockIdx.x / gridDim.x);
+        end = (int)(T * (blockIdx.x + 1) / gridDim.x);
+      }
     } else {
       pos = (int)blockIdx.x;
       end = g.ntm * g.ntn;
