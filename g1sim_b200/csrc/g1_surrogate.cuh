@@ -37,24 +37,47 @@ __global__ void __launch_bounds__(kLossThreads) sur_loss_kernel(int B, int D, co
   const int ld = D + 2;
   const int c = threadIdx.x % D;
   const float wc = w[c];
+  const int total = rows * D;
   float acc = 0.0f, l = 0.0f;
-  for (int i = threadIdx.x; i < rows * D; i += kLossThreads) {
-    const int r = i / D;
-    const size_t gi = (size_t)(r0 + r) * D + c;
-    const float e = Y[gi] - T[gi];
-    l += wc * e * e;
-    const float g = 2.0f * wc * e / (float)B;
-    acc += g;
-    const __nv_bfloat16 gb = __float2bfloat16_rn(g);
-    dY[gi] = gb;
-    tile[r * ld + c] = gb;
+  // eight rows' loads in flight per thread before their arithmetic
+  for (int i0 = threadIdx.x; i0 < total; i0 += 8 * kLossThreads) {
+    float e[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * kLossThreads;
+      const size_t gi = (size_t)(r0 + i / D) * D + c;
+      e[u] = i < total ? Y[gi] - T[gi] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * kLossThreads;
+      if (i >= total) continue;
+      const int r = i / D;
+      l += wc * e[u] * e[u];
+      const float g = 2.0f * wc * e[u] / (float)B;
+      acc += g;
+      const __nv_bfloat16 gb = __float2bfloat16_rn(g);
+      dY[(size_t)(r0 + r) * D + c] = gb;
+      tile[r * ld + c] = gb;
+    }
   }
   red[threadIdx.x] = acc;
   for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
   if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = l;
   __syncthreads();
-  for (int i = threadIdx.x; i < D * rows; i += kLossThreads) {
-    const int cc = i / rows, r = i - cc * rows;
+  // transposed copy, eight consecutive rows of one column (16 bytes) per store
+  // where a full, 16-byte aligned group of eight rows exists
+  const bool vec = (B & 7) == 0 && (reinterpret_cast<uintptr_t>(dYt) & 15) == 0;
+  const int groups = vec ? rows / 8 : 0;
+  for (int i = threadIdx.x; i < D * groups; i += kLossThreads) {
+    const int cc = i / groups, r = (i - cc * groups) * 8;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = tile[(r + u) * ld + cc];
+    *reinterpret_cast<uint4*>(dYt + (size_t)cc * B + r0 + r) = *reinterpret_cast<const uint4*>(v);
+  }
+  for (int i = threadIdx.x; i < D * (rows - 8 * groups); i += kLossThreads) {
+    const int cc = i / (rows - 8 * groups), r = 8 * groups + i % (rows - 8 * groups);
     dYt[(size_t)cc * B + r0 + r] = tile[r * ld + cc];
   }
   if (threadIdx.x < D) {

@@ -30,6 +30,8 @@
     100 ms horizon well below the policy's unrefined targets (measured 47 %
     lower; the exact adjoint's gradient on the same budget: 51 %).
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 import torch
@@ -154,6 +156,32 @@ def test_linear_silu_rejects_aliasing_and_bad_shapes():
         S.linear_silu_bwd(A, W, Z, A)
     with pytest.raises(RuntimeError, match="M % 128"):
         S.linear_silu(A[:96], W, None, torch.zeros(96, 64, dtype=torch.bfloat16, device=DEV))
+
+
+@pytest.mark.parametrize("B", [4096, 300])
+def test_loss_kernel(B):
+    """Weighted MSE, its BF16 gradient and transpose, bias-gradient sums and
+    the loss, against torch: 4,096 rows (16-byte transposed stores) and 300
+    (a partial block, the element-wise fallback)."""
+    g = torch.Generator(device=DEV).manual_seed(B)
+    Y = torch.randn(B, 64, device=DEV, generator=g)
+    T = torch.randn(B, 64, device=DEV, generator=g)
+    w = torch.rand(64, device=DEV, generator=g)
+    dY = torch.zeros(B, 64, dtype=torch.bfloat16, device=DEV)
+    dYt = torch.zeros(64, B, dtype=torch.bfloat16, device=DEV)
+    db = torch.full((64,), 0.5, device=DEV)
+    loss = torch.full((1,), 2.0, device=DEV)
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    _lib.check(_lib.lib().g1b_sur_loss(B, 64, p(Y), p(T), p(w), p(dY), p(dYt), p(db), p(loss),
+                                       C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)), "g1b_sur_loss")
+    torch.cuda.synchronize()
+    e = Y - T
+    grad = 2.0 * w * e / B
+    assert torch.equal(dY, grad.to(torch.bfloat16))
+    assert torch.equal(dYt, dY.T)
+    assert torch.allclose(db, grad.sum(0) + 0.5, rtol=1e-5, atol=1e-6)
+    ref = (w.double() * e.double() ** 2).sum() / B + 2.0
+    assert abs(loss.item() - ref.item()) <= 1e-5 * abs(ref.item())
 
 
 def cpu_reference(sur, X, T):
