@@ -25,7 +25,8 @@
 //            waits until the MMAs have released the stage, then copies the
 //            A chunk (128 x 64) and the B chunk (Nt x 64) with
 //            cp.async.bulk.tensor (tensor maps over this GPU's memory, each
-//            copy into this CTA only) into the ring (EpiCfg::kStages deep); the copies
+//            copy into this CTA only) into the ring (EpiCfg::kStages stages of the
+//            widest tile, more for narrower ones); the copies
 //            complete on the stage's `full` mbarrier (transaction bytes);
 //   warp 1   (one lane) MMA issuer: per chunk waits on `full`, issues four
 //            tcgen05.mma (M 128, N Nt, K 16) into one of two tensor-memory
@@ -77,6 +78,7 @@ constexpr uint32_t kGemmStageBytes = kGemmABytes + kGemmBBytes;
 constexpr uint32_t kGemmAccCols = 256;  // one accumulator; two of them fill the 512 TMEM columns
 constexpr uint32_t kEpiBiasBytes = 512;  // per epilogue warp: the bias of its columns of a tile
 constexpr int kGemmMaxEpiWarps = 12;
+constexpr int kGemmMaxRing = 8;  // ring stages at most (narrow tiles)
 
 // Per mode: operand ring depth, epilogue warps (a multiple of four: 2 or 3
 // per TMEM lane quarter, so 2 or 3 per SM sub-partition to hide each other's
@@ -529,19 +531,25 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ GemmOutMaps om, GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t gsm[];
-  constexpr int kStages = EpiCfg<kMode>::kStages;
-  __shared__ uint64_t full[kStages], empty[kStages], accf[2], acce[2], drain, zbar[2 * kGemmMaxEpiWarps];
+  // The ring holds EpiCfg::kStages stages of the widest tile (Nt = 256); a
+  // narrower tile (the output layer's Nt = 64) packs more, smaller stages
+  // into the same bytes, so more of its operand stream is in flight.
+  constexpr uint32_t kRingBytes = (uint32_t)EpiCfg<kMode>::kStages * kGemmStageBytes;
+  const uint32_t stage_bytes = kGemmABytes + (uint32_t)g.Nt * kGemmKC * 2;  // a multiple of 2 KB
+  const uint32_t nst = kRingBytes / stage_bytes < (uint32_t)kGemmMaxRing ? kRingBytes / stage_bytes
+                                                                         : (uint32_t)kGemmMaxRing;
+  __shared__ uint64_t full[kGemmMaxRing], empty[kGemmMaxRing], accf[2], acce[2], drain, zbar[2 * kGemmMaxEpiWarps];
   __shared__ uint32_t tslot;
   __shared__ int abort_flag;
   volatile int* abort_v = &abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t base0 = tc::smem_u32(gsm);
   const uint32_t sbase = (base0 + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
-  const uint32_t ebase0 = sbase + (uint32_t)kStages * kGemmStageBytes;  // epilogue staging
+  const uint32_t ebase0 = sbase + kRingBytes;  // epilogue staging
   const int ntiles = g.ntm * g.ntn;
   const uint32_t btx = (uint32_t)g.Nt * kGemmKC * 2;  // B bytes per chunk
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (uint32_t s = 0; s < nst; ++s) {
       tc::mbar_init(tc::smem_u32(&full[s]), 1);
       tc::mbar_init(tc::smem_u32(&empty[s]), 1);
     }
@@ -577,13 +585,13 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
       GemmWork w;
       while (ok && sched.next(g, w)) {
         for (int c = 0; c < w.nk; ++c) {
-          const int s = (int)(it % kStages);
-          const uint32_t r = it / kStages;
+          const int s = (int)(it % nst);
+          const uint32_t r = it / nst;
           if (r > 0 && !gemm_wait(tc::smem_u32(&empty[s]), (r - 1) & 1, abort_v)) {
             ok = false;
             break;
           }
-          const uint32_t st = sbase + (uint32_t)s * kGemmStageBytes;
+          const uint32_t st = sbase + (uint32_t)s * stage_bytes;
           const uint32_t bar = tc::smem_u32(&full[s]);
           const int kx = (w.k0 + c) * kGemmKC;
           tc::mbar_expect_tx(bar, kGemmABytes + btx);
@@ -593,8 +601,8 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
         }
       }
       // every copy issued has landed before the CTA may exit
-      for (int s = 0; s < kStages; ++s) {
-        const uint32_t n_s = it > (uint32_t)s ? (it - (uint32_t)s - 1) / kStages + 1 : 0;
+      for (uint32_t s = 0; s < nst; ++s) {
+        const uint32_t n_s = it > s ? (it - s - 1) / nst + 1 : 0;
         if (n_s > 0 && !tc::mbar_wait(tc::smem_u32(&full[s]), (n_s - 1) & 1)) ok = false;
       }
     }
@@ -615,14 +623,14 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
         tc::tc_fence_after();
         const uint32_t d = tmem + (uint32_t)b * kGemmAccCols;
         for (int c = 0; c < w.nk; ++c, ++it) {
-          const int s = (int)(it % kStages);
-          const uint32_t r = it / kStages;
+          const int s = (int)(it % nst);
+          const uint32_t r = it / nst;
           if (!gemm_wait(tc::smem_u32(&full[s]), r & 1, abort_v)) {
             ok = false;
             break;
           }
           tc::tc_fence_after();
-          const uint32_t st = sbase + (uint32_t)s * kGemmStageBytes;
+          const uint32_t st = sbase + (uint32_t)s * stage_bytes;
 #pragma unroll
           for (int kk = 0; kk < kGemmKC / 16; ++kk)
             tc::mma_bf16(d, gemm_desc_sw128(st, kk), gemm_desc_sw128(st + kGemmABytes, kk), idesc,
