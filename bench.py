@@ -548,16 +548,15 @@ def surrogate_bench(device, train_steps, world):
     g = torch.Generator(device=device).manual_seed(0)
     idx = torch.randint(0, X.shape[0], (SUR_BATCH,), generator=g, device=device)
     xb, tb = X[idx].contiguous(), T[idx].contiguous()
-    xt = xb.T.contiguous()
     sur.forward(xb, keep=True)
-    l0 = float(sur.backward(xb, xt, tb).item())
+    l0 = float(sur.backward(xb, tb).item())
     # timed training steps (the same minibatch each step keeps the timed region to the kernels):
     # the CUDA graph of the step the library's training loop replays, and the eager launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    tg = sur.capture_train_step(xb, xt, tb, lr=1e-3)
+    tg = sur.capture_train_step(xb, tb, lr=1e-3)
     timed = {}
-    for name, fn in (("graph", tg.step), ("eager", lambda: sur.train_step(xb, xt, tb, lr=1e-3))):
+    for name, fn in (("graph", tg.step), ("eager", lambda: sur.train_step(xb, tb, lr=1e-3))):
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
@@ -679,11 +678,13 @@ def refinement_bench(sur, device, n=4096, H=50, iters=10):
 def gemm_bench(device, rows, steps, warmup):
     """The surrogate's layer products alone, rows x 512 x 512, each timed over
     `steps` calls with CUDA events: the plain product C = A W^T + b (FP32 C,
-    g1b_gemm_bf16), the fused hidden layer of training (FP16 Z, BF16 H and
-    H^T) and of inference (BF16 H only), the fused backward through SiLU (FP16
-    Z in; BF16 dZ and dZ^T, bias-gradient sums) and the weight gradient (K = rows split
-    over tiles, atomic FP32 sums).  hbm_gbs: algorithmic bytes (operands read
-    once, outputs written once) per call over its time."""
+    g1b_gemm_bf16), the fused hidden layer of training (FP16 Z, BF16 H) and
+    of inference (BF16 H only), the fused backward through SiLU (FP16 Z in;
+    BF16 dZ, bias-gradient sums) and the weight gradient (K = rows split over
+    tiles, atomic FP32 sums) from the row-major activations (MN-major tiles,
+    the training step's form) and from transposed copies (K-major tiles).
+    hbm_gbs: algorithmic bytes (operands read once, outputs written once) per
+    call over its time."""
     import torch
     from g1sim_b200 import surrogate as S
     g = torch.Generator(device=device).manual_seed(0)
@@ -716,10 +717,13 @@ def gemm_bench(device, rows, steps, warmup):
     flops = 2.0 * rows * 512 * 512
     el = rows * 512
     cases = [("store", lambda: S.gemm(A_, W, C_, bias=b), el * (2 + 4)),
-             ("silu_forward_training", lambda: S.linear_silu(A_, W, b, H, Z=Z, Ht=Ht), el * (2 + 2 + 2 + 2)),
+             ("silu_forward_training", lambda: S.linear_silu(A_, W, b, H, Z=Z), el * (2 + 2 + 2)),
              ("silu_forward_inference", lambda: S.linear_silu(A_, W, b, H), el * (2 + 2)),
-             ("silu_backward", lambda: S.linear_silu_bwd(A_, W, Z, H, dHt=Ht, db=db), el * (2 + 2 + 2 + 2)),
-             ("weight_gradient", lambda: S.gemm(At, Ht, Cw, splits=splits), el * (2 + 2))]
+             ("silu_backward", lambda: S.linear_silu_bwd(A_, W, Z, H, db=db), el * (2 + 2 + 2)),
+             # the training step's form: MN-major tiles of the row-major activations
+             ("weight_gradient", lambda: (Cw.zero_(), S.gemm_atb(A_, H, Cw)), el * (2 + 2)),
+             # the same product from transposed copies (K-major tiles)
+             ("weight_gradient_k_major", lambda: S.gemm(At, Ht, Cw, splits=splits), el * (2 + 2))]
     modes = {}
     for name, fn, nbytes in cases:
         ms = timed(fn)

@@ -100,6 +100,7 @@ def lib():
                                 _vp]
     L.g1b_gemm_status.argtypes = [C.POINTER(C.c_int)]
     L.g1b_gemm_bf16_acc.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]
+    L.g1b_gemm_bf16_atb_acc.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]
     L.g1b_sur_linear_silu.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int,
                                                        _vp, C.c_int, _vp]
     L.g1b_sur_linear_silu_bwd.argtypes = [C.c_int] * 3 + [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,

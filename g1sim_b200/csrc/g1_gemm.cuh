@@ -12,6 +12,12 @@
 //                   H (BF16) = silu(z), Ht (BF16, transposed [N][M], nullable)
 //     kGemmSiluBwd  g = acc * silu'(Zin) (Zin FP16); H (BF16) = g, Ht = g
 //                   transposed (nullable), db[N] += column sums of g (nullable)
+// With GemmArgs::mn the operands are instead A[K x M] and B[K x N], both
+// row-major (C = A^T . B, the weight gradient dW = dZ^T . H from the
+// activations as the forward and backward layers store them, with no
+// transposed copies): the TMA boxes are 64 K rows x 64 columns and the MMAs
+// read them as MN-major tiles.  A row tile may then extend past M (the boxes
+// beyond it are zero-filled and the atomic epilogue skips those rows).
 // The pre-activation Z is kept in FP16 (11 significant bits, eight times
 // finer than the BF16 activations; |z| clamped to 65000, where silu' is
 // 0 or 1) only for the SiLU derivative of the backward pass.
@@ -122,6 +128,8 @@ struct GemmArgs {
   __half* Z;  // silu: the pre-activation out (nullable); silu_bwd: in
   int ldz;
   float* db;  // silu_bwd: column sums, nullable
+  int M;      // rows of C: the atomic epilogue adds no row at or beyond M (a partial last row tile)
+  int mn;     // 1: A given as [K][M] and B as [K][N], row-major (MN-major operands, C += A^T B)
   int* err;
 };
 
@@ -149,6 +157,17 @@ __device__ __forceinline__ uint64_t gemm_desc_sw128(uint32_t tile, int kk) {
   const uint32_t a = tile + (uint32_t)kk * 32u;
   return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) |
          (2ull << 61);
+}
+
+// Shared-memory descriptor of an MN-major tile (SWIZZLE_128B) at K step kk:
+// each TMA box is 64 K rows of 64 M (or N) values (128 B per row, 8 KB per
+// box), so the 8-row atoms of one box are 1024 B apart (stride offset) and
+// the boxes, i.e. the 64-wide blocks along M or N, 8 KB apart (leading
+// offset); a K step of 16 rows starts 2048 B further on.
+__device__ __forceinline__ uint64_t gemm_desc_mn128(uint32_t tile, int kk) {
+  const uint32_t a = tile + (uint32_t)kk * 2048u;
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)(8192u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
 }
 
 // 2-D tiled TMA load of the box at (x, y) (x the inner coordinate, a
@@ -477,7 +496,7 @@ __device__ __forceinline__ bool gemm_epilogue(const GemmArgs& g, const CUtensorM
         }
       }
       if constexpr (kMode == kGemmAtomic) {
-        direct_f32<true>(g.C + (size_t)row * g.ldc + col, v, nb);
+        if (row < g.M) direct_f32<true>(g.C + (size_t)row * g.ldc + col, v, nb);
       } else {
         float hv[32];  // the BF16 output's values
 #pragma unroll
@@ -595,8 +614,15 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
           const uint32_t bar = tc::smem_u32(&full[s]);
           const int kx = (w.k0 + c) * kGemmKC;
           tc::mbar_expect_tx(bar, kGemmABytes + btx);
-          tma_load_2d(st, &tmA, kx, w.m * 128, bar);
-          tma_load_2d(st + kGemmABytes, &tmB, kx, w.n * g.Nt, bar);
+          if (g.mn) {  // 64-column boxes of the row-major [K][M] and [K][N] operands
+            tma_load_2d(st, &tmA, w.m * 128, kx, bar);
+            tma_load_2d(st + 8192u, &tmA, w.m * 128 + 64, kx, bar);  // beyond M: zero fill
+            for (int b = 0; b < g.Nt / 64; ++b)
+              tma_load_2d(st + kGemmABytes + 8192u * (uint32_t)b, &tmB, w.n * g.Nt + 64 * b, kx, bar);
+          } else {
+            tma_load_2d(st, &tmA, kx, w.m * 128, bar);
+            tma_load_2d(st + kGemmABytes, &tmB, kx, w.n * g.Nt, bar);
+          }
           ++it;
         }
       }
@@ -608,7 +634,8 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {  // ---- MMA issuer
-      const uint32_t idesc = tc::idesc_bf16(128, g.Nt);
+      // bits 15 and 16: A and B MN-major
+      const uint32_t idesc = tc::idesc_bf16(128, g.Nt) | (g.mn ? (3u << 15) : 0u);
       uint32_t it = 0;
       int j = 0;  // work units of this CTA
       GemmSched<kMode> sched(g);
@@ -632,9 +659,11 @@ __global__ void __launch_bounds__(EpiCfg<kMode>::kThreads, 1)
           tc::tc_fence_after();
           const uint32_t st = sbase + (uint32_t)s * stage_bytes;
 #pragma unroll
-          for (int kk = 0; kk < kGemmKC / 16; ++kk)
-            tc::mma_bf16(d, gemm_desc_sw128(st, kk), gemm_desc_sw128(st + kGemmABytes, kk), idesc,
-                         (c > 0 || kk > 0) ? 1u : 0u);
+          for (int kk = 0; kk < kGemmKC / 16; ++kk) {
+            const uint64_t ad = g.mn ? gemm_desc_mn128(st, kk) : gemm_desc_sw128(st, kk);
+            const uint64_t bd = g.mn ? gemm_desc_mn128(st + kGemmABytes, kk) : gemm_desc_sw128(st + kGemmABytes, kk);
+            tc::mma_bf16(d, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+          }
           tc::mma_commit(tc::smem_u32(&empty[s]));
         }
         if (!ok) break;

@@ -55,22 +55,36 @@ static int map_bf16_operand(CUtensorMap* m, const void* p, int rows, int cols, i
 }
 
 // Shape checks, tensor maps and the persistent launch of gemm_kernel<kMode>
-// (one CTA per SM, at most one per tile).
+// (one CTA per SM, at most one per tile).  mn: A is [K][M] and B [K][N]
+// (row-major, C = A^T B), loaded in 64 x 64 boxes as MN-major tiles.
 template <int kMode>
 static int gemm_run(const char* what, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
-                    GemmArgs g, cudaStream_t st, bool clear_c = false) {
+                    GemmArgs g, cudaStream_t st, bool clear_c = false, bool mn = false) {
   if (M <= 0 || N <= 0 || K <= 0 || !A || !B) return failf("%s: invalid arguments", what);
   const int Nt = N <= kGemmMaxN ? N : kGemmMaxN;
-  if (M % 128 || N % 16 || N % Nt || K % kGemmKC)
-    return failf("%s: needs M %% 128 == 0, N %% 16 == 0 (and N %% 256 == 0 above 256), K %% 64 == 0", what);
-  if (lda % 8 || ldb % 8 || lda < K || ldb < K || (((uintptr_t)A | (uintptr_t)B) & 15))
-    return failf("%s: lda, ldb multiples of 8 and >= K, 16-byte aligned operands", what);
+  if (mn) {
+    if (M % 16 || N % 64 || N % Nt || K % kGemmKC)
+      return failf("%s: needs M %% 16 == 0, N %% 64 == 0 (and N %% 256 == 0 above 256), K %% 64 == 0", what);
+    if (lda % 8 || ldb % 8 || lda < M || ldb < N || (((uintptr_t)A | (uintptr_t)B) & 15))
+      return failf("%s: lda >= M, ldb >= N, both multiples of 8, 16-byte aligned operands", what);
+  } else {
+    if (M % 128 || N % 16 || N % Nt || K % kGemmKC)
+      return failf("%s: needs M %% 128 == 0, N %% 16 == 0 (and N %% 256 == 0 above 256), K %% 64 == 0", what);
+    if (lda % 8 || ldb % 8 || lda < K || ldb < K || (((uintptr_t)A | (uintptr_t)B) & 15))
+      return failf("%s: lda, ldb multiples of 8 and >= K, 16-byte aligned operands", what);
+  }
   if (g.Ht && (g.ldt % 8 || ((uintptr_t)g.Ht & 15)))
     return failf("%s: the transposed output needs ldt %% 8 == 0 and 16-byte alignment", what);
   CUtensorMap ma, mb;
   GemmOutMaps om;
   memset(&om, 0, sizeof(om));
-  if (map_bf16_operand(&ma, A, M, K, lda, 128) || map_bf16_operand(&mb, B, N, K, ldb, Nt)) return -1;
+  if (mn) {
+    if (gemm_map(&ma, A, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, K, M, lda, 64, kGemmKC, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        gemm_map(&mb, B, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, K, N, ldb, 64, kGemmKC, CU_TENSOR_MAP_SWIZZLE_128B))
+      return -1;
+  } else if (map_bf16_operand(&ma, A, M, K, lda, 128) || map_bf16_operand(&mb, B, N, K, ldb, Nt)) {
+    return -1;
+  }
   // the f map: FP32 C (store), or the FP16 pre-activation (silu out, silu_bwd in)
   if (kMode == kGemmStore &&
       gemm_map(&om.f, g.C, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, M, N, g.ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B))
@@ -88,7 +102,9 @@ static int gemm_run(const char* what, int M, int N, int K, const void* A, int ld
   if (e != cudaSuccess) return cuda_fail(e, "gemm: error flag");
   if (clear_c && (e = cudaMemset2DAsync(g.C, (size_t)g.ldc * 4, 0, (size_t)N * 4, M, st)) != cudaSuccess)
     return cuda_fail(e, "gemm: clear C");
-  g.ntm = M / 128;
+  g.ntm = (M + 127) / 128;
+  g.M = M;
+  g.mn = mn ? 1 : 0;
   g.ntn = N / Nt;
   g.nk = K / kGemmKC;
   g.Nt = Nt;
@@ -142,6 +158,17 @@ int g1b_gemm_bf16_acc(int M, int N, int K, const void* A, int lda, const void* B
   g.C = C;
   g.ldc = ldc;
   return gemm_run<kGemmAtomic>("gemm_bf16_acc", M, N, K, A, lda, B, ldb, g, static_cast<cudaStream_t>(stream));
+}
+
+int g1b_gemm_bf16_atb_acc(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                          void* stream) {
+  if (!C || ldc < N || ldc % 4 || ((uintptr_t)C & 15))
+    return fail("gemm_bf16_atb_acc: C needs ldc >= N, ldc % 4 == 0, 16-byte alignment");
+  GemmArgs g{};
+  g.C = C;
+  g.ldc = ldc;
+  return gemm_run<kGemmAtomic>("gemm_bf16_atb_acc", M, N, K, A, lda, B, ldb, g, static_cast<cudaStream_t>(stream),
+                               false, true);
 }
 
 int g1b_sur_linear_silu(int M, int N, int K, const void* A, int lda, const void* W, int ldw, const float* bias,
@@ -199,7 +226,7 @@ static int grid_1d(size_t n, int block) {
 
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream) {
-  if (B <= 0 || D <= 0 || !Y || !T || !w || !dY || !dYt || !db || !loss) return fail("sur_loss: invalid arguments");
+  if (B <= 0 || D <= 0 || !Y || !T || !w || !dY || !db || !loss) return fail("sur_loss: invalid arguments");
   if (D % 8 || kLossThreads % D) return fail("sur_loss: D must divide 256 and be a multiple of 8");
   const int blocks = (B + kLossRows - 1) / kLossRows;
   sur_loss_kernel<<<blocks, kLossThreads, (size_t)kLossRows * (D + 2) * 2, static_cast<cudaStream_t>(stream)>>>(

@@ -58,26 +58,27 @@ __global__ void __launch_bounds__(kLossThreads) sur_loss_kernel(int B, int D, co
       acc += g;
       const __nv_bfloat16 gb = __float2bfloat16_rn(g);
       dY[(size_t)(r0 + r) * D + c] = gb;
-      tile[r * ld + c] = gb;
+      if (dYt) tile[r * ld + c] = gb;
     }
   }
   red[threadIdx.x] = acc;
   for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
   if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = l;
   __syncthreads();
-  // transposed copy, eight consecutive rows of one column (16 bytes) per store
-  // where a full, 16-byte aligned group of eight rows exists
+  // transposed copy (dYt nullable), eight consecutive rows of one column
+  // (16 bytes) per store where a full, 16-byte aligned group of eight rows exists
   const bool vec = (B & 7) == 0 && (reinterpret_cast<uintptr_t>(dYt) & 15) == 0;
   const int groups = vec ? rows / 8 : 0;
-  for (int i = threadIdx.x; i < D * groups; i += kLossThreads) {
+  const int tail = dYt ? rows - 8 * groups : 0;
+  for (int i = threadIdx.x; dYt && i < D * groups; i += kLossThreads) {
     const int cc = i / groups, r = (i - cc * groups) * 8;
     __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) v[u] = tile[(r + u) * ld + cc];
     *reinterpret_cast<uint4*>(dYt + (size_t)cc * B + r0 + r) = *reinterpret_cast<const uint4*>(v);
   }
-  for (int i = threadIdx.x; i < D * (rows - 8 * groups); i += kLossThreads) {
-    const int cc = i / (rows - 8 * groups), r = 8 * groups + i % (rows - 8 * groups);
+  for (int i = threadIdx.x; i < D * tail; i += kLossThreads) {
+    const int cc = i / tail, r = 8 * groups + i % tail;
     dYt[(size_t)cc * B + r0 + r] = tile[r * ld + cc];
   }
   if (threadIdx.x < D) {

@@ -66,6 +66,17 @@ def gemm(A, B, C_, bias=None, splits=1, acc=False):
                                         _p(bias), splits, _st(A.device)), "g1b_gemm_bf16")
 
 
+def gemm_atb(A, B, C_):
+    """C += A^T @ B: A [K, M], B [K, N] BF16 row-major, C [M, N] FP32, K split
+    over the SMs (tcgen05 kernel reading MN-major tiles): the weight gradient
+    dW += dZ^T H from the activations as the layers store them."""
+    K, M_ = A.shape
+    N = B.shape[1]
+    assert B.shape[0] == K and C_.shape == (M_, N) and A.dtype == B.dtype == torch.bfloat16
+    _lib.check(_lib.lib().g1b_gemm_bf16_atb_acc(M_, N, K, _p(A), A.stride(0), _p(B), B.stride(0), _p(C_),
+                                                C_.stride(0), _st(A.device)), "g1b_gemm_bf16_atb_acc")
+
+
 def linear_silu(A, W, bias, H, Z=None, Ht=None):
     """One hidden layer, fused: z = A @ W^T + bias; H = bf16(silu(z)) [M, N];
     Z = z (FP16 [M, N], optional: the backward pass's SiLU derivative);
@@ -126,7 +137,7 @@ class Surrogate:
         self.Wt = [torch.empty(w.shape[1], w.shape[0], dtype=torch.bfloat16, device=device) for w in self.W]
         # every gradient and the loss in one buffer, zeroed by one launch per backward pass
         # (the weight gradients are summed into it by split-K GEMMs)
-        shapes = [(max(w.shape[0], 128), w.shape[1]) for w in self.W] + [tuple(b.shape) for b in self.b] + [(1,)]
+        shapes = [tuple(w.shape) for w in self.W] + [tuple(b.shape) for b in self.b] + [(1,)]
         sizes = [int(np.prod(sh)) for sh in shapes]
         self._grad = torch.zeros(sum(sizes), device=device)
         views, off = [], 0
@@ -165,14 +176,10 @@ class Surrogate:
                 Z=[None] + [torch.empty(B, DIMS[i], dtype=torch.float16, device=d) for i in range(1, 5)] +
                   [torch.empty(B, DIMS[5], device=d)],
                 H=[None] + [torch.empty(B, DIMS[i], dtype=bf, device=d) for i in range(1, 5)],
-                Ht=[None] + [torch.empty(DIMS[i], B, dtype=bf, device=d) for i in range(1, 5)],
                 dX=torch.empty(B, NIN, device=d),
                 dY=torch.zeros(B, 64, device=d),
                 dZ=torch.empty(B, 512, dtype=bf, device=d),
-                dZ2=torch.empty(B, 512, dtype=bf, device=d),
-                dZt=torch.empty(512, B, dtype=bf, device=d),
-                # the output layer's dY transposed, padded to 128 rows (rows 64-127 stay zero)
-                dYt=torch.zeros(128, B, dtype=bf, device=d))
+                dZ2=torch.empty(B, 512, dtype=bf, device=d))
         return self._ws[B]
 
     def features(self, qpos, qvel, anchor, ctrl, X, Xt=None, raw=None, mu=None, dmass=None):
@@ -190,39 +197,36 @@ class Surrogate:
         L = _lib.lib()
         h = X
         for i in range(4):  # hidden layers: GEMM, bias and SiLU in one kernel
-            linear_silu(h, self.Wb[i], self.b[i], w["H"][i + 1], Z=w["Z"][i + 1] if keep else None,
-                        Ht=w["Ht"][i + 1] if keep else None)
+            linear_silu(h, self.Wb[i], self.b[i], w["H"][i + 1], Z=w["Z"][i + 1] if keep else None)
             h = w["H"][i + 1]
         gemm(h, self.Wb[4], w["Z"][5], bias=self.b[4])
         return w["Z"][5]
 
-    def backward(self, X, Xt, T, want_dx=False, weights=None):
+    def backward(self, X, T, want_dx=False, weights=None):
         """Loss of the last forward(X, keep=True) against normalised targets T
         [B, 64] (weighted MSE, per-output weights), and the gradients of every
         parameter (self.gW, self.gb); with want_dx also d loss / d X (FP32
-        [B, 128], in self.dX(B)).  Xt: X transposed [128, B]."""
+        [B, 192], in self.dX(B))."""
         B = X.shape[0]
         w = self._work(B)
         L = _lib.lib()
         st = _st(self.device)
         self._grad.zero_()  # every parameter gradient and the loss
-        dZ, dZt, dYt = w["dZ"], w["dZt"], w["dYt"]
+        dZ = w["dZ"]
         wv = self.out_w if weights is None else weights
-        # dY = d loss / d Y as BF16 [B][64] (start of dZ) and [64][B] (rows 0-63 of dYt)
-        _lib.check(L.g1b_sur_loss(B, 64, _p(w["Z"][5]), _p(T), _p(wv), _p(dZ), _p(dYt), _p(self.gb[4]),
+        # dY = d loss / d Y as BF16 [B][64] (the start of dZ)
+        _lib.check(L.g1b_sur_loss(B, 64, _p(w["Z"][5]), _p(T), _p(wv), _p(dZ), None, _p(self.gb[4]),
                                   _p(self.loss_buf), st), "sur_loss")
         bufs = [w["dZ"], w["dZ2"]]  # the layer's dZ and the previous layer's, alternating
         for i in range(4, -1, -1):
             Din, Dout = DIMS[i], DIMS[i + 1]
             dz = bufs[i & 1].view(-1)[:B * Dout].view(B, Dout)
-            rows = max(Dout, 128)
-            hin_t = w["Ht"][i] if i > 0 else Xt
             # dW_i = dZ_i^T . H_{i-1} (the batch split over the SMs, summed into the zeroed gradient)
-            gemm((dYt if i == 4 else dZt)[:rows], hin_t, self.gW[i][:rows], acc=True)
+            gemm_atb(dz, w["H"][i] if i > 0 else X, self.gW[i])
             if i > 0:
                 # dZ_{i-1} = (dZ_i . W_i) * SiLU'(Z_{i-1}), its transpose and bias gradient, one kernel
                 nxt = bufs[(i - 1) & 1].view(-1)[:B * Din].view(B, Din)
-                linear_silu_bwd(dz, self.Wt[i], w["Z"][i], nxt, dHt=dZt, db=self.gb[i - 1])
+                linear_silu_bwd(dz, self.Wt[i], w["Z"][i], nxt, db=self.gb[i - 1])
             elif want_dx:
                 gemm(dz, self.Wt[0], w["dX"])
         return self.loss_buf
@@ -258,17 +262,17 @@ class Surrogate:
         _lib.check(_lib.lib().g1b_sur_adam_cast(5, self._layers, _p(self.opt_step), _p(self.lr_dev), b1, b2, eps,
                                                 _st(self.device)), "sur_adam_cast")
 
-    def train_step(self, X, Xt, T, lr=1e-3):
+    def train_step(self, X, T, lr=1e-3):
         self.forward(X, keep=True)
-        loss = self.backward(X, Xt, T)
+        loss = self.backward(X, T)
         self.adam(lr)
         return loss
 
-    def capture_train_step(self, X, Xt, T, lr):
-        """A CUDA graph of train_step on the fixed buffers X, Xt, T (write the
+    def capture_train_step(self, X, T, lr):
+        """A CUDA graph of train_step on the fixed buffers X, T (write the
         next minibatch into them, then call the returned step(lr)).  Runs one
         eager training step first (with `lr`), which prepares every kernel."""
-        return TrainGraph(self, X, Xt, T, lr)
+        return TrainGraph(self, X, T, lr)
 
     def integrate(self, Y, qpos, qvel, dt):
         n = qpos.shape[1]
@@ -282,17 +286,17 @@ class TrainGraph:
     without the host in between.  The learning rate and Adam's step count are
     read from device memory, so each replay uses the current ones."""
 
-    def __init__(self, sur, X, Xt, T, lr):
+    def __init__(self, sur, X, T, lr):
         self.sur = sur
         dev = sur.device
         s = torch.cuda.Stream(dev)
         s.wait_stream(torch.cuda.current_stream(dev))
         with torch.cuda.stream(s):
-            sur.train_step(X, Xt, T, lr=lr)  # a real step, which also prepares the kernels
+            sur.train_step(X, T, lr=lr)  # a real step, which also prepares the kernels
         torch.cuda.current_stream(dev).wait_stream(s)
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph, stream=s):
-            self.loss = sur.train_step(X, Xt, T, lr=None)
+            self.loss = sur.train_step(X, T, lr=None)
         sur.step_n -= 1  # the capture ran no step
 
     def step(self, lr=None):
@@ -379,17 +383,15 @@ def train(sur, F, A, steps, batch=65536, lr=1e-3, seed=0, log_every=0):
     dev = X.device
     g = torch.Generator(device=dev).manual_seed(seed)
     xb = torch.empty(batch, NIN, dtype=torch.bfloat16, device=dev)
-    xt = torch.empty(NIN, batch, dtype=torch.bfloat16, device=dev)
     tb = torch.empty(batch, T.shape[1], device=dev)
     hist, tg = [], None
     for k in range(steps):
         idx = torch.randint(0, N, (batch,), generator=g, device=dev)
         torch.index_select(X, 0, idx, out=xb)
-        xt.copy_(xb.T)
         torch.index_select(T, 0, idx, out=tb)
         cur_lr = lr * (0.1 ** (k / max(steps, 1)))
         if tg is None:
-            tg = sur.capture_train_step(xb, xt, tb, cur_lr)
+            tg = sur.capture_train_step(xb, tb, cur_lr)
             loss = tg.loss
         else:
             loss = tg.step(cur_lr)

@@ -262,6 +262,14 @@ int g1b_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
  * into buffers the caller zeroes once for several products. */
 int g1b_gemm_bf16_acc(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                       void* stream);
+/* C[M x N] += A[K x M]^T . B[K x N] with A and B row-major (K the rows):
+ * the weight gradient dW += dZ^T . H read from the activations as the layers
+ * store them (no transposed copies), K shared evenly by the SMs as in
+ * g1b_gemm_bf16_acc.  M % 16 == 0, N % 64 == 0 (N % 256 == 0 above 256),
+ * K % 64 == 0, lda >= M and ldb >= N multiples of 8, ldc a multiple of 4
+ * and >= N, 16-byte aligned pointers. */
+int g1b_gemm_bf16_atb_acc(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                          void* stream);
 /* One hidden layer of the surrogate in one GEMM with a fused epilogue
  * (same shape rules; ldh and ldz multiples of 8, ldt >= M):
  *   z = A . W^T + bias (W [N x K]); Z = z (FP16 [M][ldz], |z| clamped to
@@ -293,8 +301,8 @@ typedef struct g1b_sur_layer {
 int g1b_sur_adam_cast(int nl, const g1b_sur_layer* layers, const int* step, const float* lr, float b1, float b2,
                       float eps, void* stream);
 /* Element-wise kernels of the surrogate: weighted MSE and its gradient
- * (adds into db and loss; D divides 256 and is a multiple of 8), BF16
- * weight copies. */
+ * dY [B][D] (BF16; dYt, its transpose [D][B], nullable; adds into db and
+ * loss; D divides 256 and is a multiple of 8), BF16 weight copies. */
 int g1b_sur_loss(int B, int D, const float* Y, const float* T, const float* w, void* dY, void* dYt, float* db,
                  float* loss, void* stream);
 int g1b_sur_cast(int rows, int cols, const float* W, void* Wb, void* Wt, void* stream);

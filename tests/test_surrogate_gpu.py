@@ -89,6 +89,45 @@ def test_gemm_many_tiles_per_cta(M_, N, K, splits):
     assert err < 1e-5, err
 
 
+@pytest.mark.parametrize("M_,N,K", [(512, 512, 4096), (512, 512, 65536), (64, 512, 8192), (512, 192, 2048),
+                                    (208, 64, 256), (1024, 768, 1024), (16, 64, 64)])
+def test_gemm_atb_matches_fp64(M_, N, K):
+    """C += A^T B from row-major A [K, M] and B [K, N] (MN-major tiles, K
+    split over the SMs): the weight-gradient shapes of the surrogate (the
+    output layer's M = 64 and the row tiles' zero-filled second half, the
+    first layer's N = 192 in three 64-column boxes, K = 65,536), a partial
+    row tile (M = 208), N above 256.  The operands sit in wider buffers whose
+    extra columns hold NaN, and C in a buffer whose extra rows and columns
+    hold 7: a read past M or N, or a write past C, shows."""
+    g = torch.Generator(device=DEV).manual_seed(M_ + 3 * N + K)
+    Abuf = torch.full((K, M_ + 16), float("nan"), dtype=torch.bfloat16, device=DEV)
+    Bbuf = torch.full((K, N + 8), float("nan"), dtype=torch.bfloat16, device=DEV)
+    A, B = Abuf[:, :M_], Bbuf[:, :N]
+    A.copy_(bf(torch.randn(K, M_, device=DEV, generator=g)))
+    B.copy_(bf(torch.randn(K, N, device=DEV, generator=g)))
+    Cbuf = torch.full((M_ + 8, N + 4), 7.0, device=DEV)
+    C_ = Cbuf[:M_, :N]
+    C0 = torch.randn(M_, N, device=DEV, generator=g)
+    C_.copy_(C0)
+    S.gemm_atb(A, B, C_)
+    torch.cuda.synchronize()
+    assert S.gemm_status() == 0
+    ref = C0.double() + A.double().T @ B.double()
+    err = ((C_.double() - ref).norm() / ref.norm()).item()
+    assert err < 1e-5, err
+    assert bool((Cbuf[M_:] == 7.0).all()) and bool((Cbuf[:, N:] == 7.0).all())
+
+
+def test_gemm_atb_rejects_bad_shapes():
+    A = torch.zeros(128, 64, dtype=torch.bfloat16, device=DEV)
+    C_ = torch.zeros(64, 48, device=DEV)
+    with pytest.raises(RuntimeError):
+        S.gemm_atb(A, torch.zeros(128, 48, dtype=torch.bfloat16, device=DEV), C_)  # N % 64
+    C_ = torch.zeros(64, 64, device=DEV)
+    with pytest.raises(RuntimeError):
+        S.gemm_atb(A[:100], torch.zeros(100, 64, dtype=torch.bfloat16, device=DEV), C_)  # K % 64
+
+
 def _bf16_close(got, ref):
     """got (BF16) is ref rounded to BF16, up to one unit in the last place
     (the FP32 sums of the kernel and the FP64 reference may straddle a
@@ -182,6 +221,12 @@ def test_loss_kernel(B):
     assert torch.allclose(db, grad.sum(0) + 0.5, rtol=1e-5, atol=1e-6)
     ref = (w.double() * e.double() ** 2).sum() / B + 2.0
     assert abs(loss.item() - ref.item()) <= 1e-5 * abs(ref.item())
+    # without the transposed copy (the training step's form): the same dY
+    dY2 = torch.zeros_like(dY)
+    _lib.check(_lib.lib().g1b_sur_loss(B, 64, p(Y), p(T), p(w), p(dY2), None, p(db), p(loss),
+                                       C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)), "g1b_sur_loss")
+    torch.cuda.synchronize()
+    assert torch.equal(dY2, dY)
 
 
 def cpu_reference(sur, X, T):
@@ -230,7 +275,7 @@ def test_training_kernels_match_cpu_restatement():
     X[:, S.NFEAT:] = 0
     T = torch.randn(B, 64, device=DEV, generator=g)
     sur.forward(X, keep=True)
-    loss = sur.backward(X, X.T.contiguous(), T, want_dx=True)
+    loss = sur.backward(X, T, want_dx=True)
     torch.cuda.synchronize()
     assert S.gemm_status() == 0
     l_ref, gW, gb, dx = cpu_reference(sur, X, T)
@@ -298,13 +343,12 @@ def test_train_graph_replays_the_eager_step():
     g = torch.Generator(device=DEV).manual_seed(6)
     X = bf(torch.randn(B, S.NIN, device=DEV, generator=g))
     X[:, S.NFEAT:] = 0
-    Xt = X.T.contiguous()
     T = torch.randn(B, 64, device=DEV, generator=g)
     a, b = S.Surrogate(DEV, seed=7), S.Surrogate(DEV, seed=7)
     lrs = [1e-3, 8e-4, 6e-4, 4e-4]
     for lr in lrs:
-        la = float(a.train_step(X, Xt, T, lr=lr).item())
-    tg = b.capture_train_step(X, Xt, T, lrs[0])  # runs the first step eagerly
+        la = float(a.train_step(X, T, lr=lr).item())
+    tg = b.capture_train_step(X, T, lrs[0])  # runs the first step eagerly
     for lr in lrs[1:]:
         lb = float(tg.step(lr).item())
     torch.cuda.synchronize()
@@ -324,10 +368,10 @@ def trained():
     S.fit_normalisation(sur, F, A)
     X, T = S.normalise(sur, F[:16384], A[:16384])
     sur.forward(X, keep=True)
-    l0 = sur.backward(X, X.T.contiguous(), T).item()
+    l0 = sur.backward(X, T).item()
     hist = S.train(sur, F, A, steps=400, batch=16384, lr=1e-3)
     sur.forward(X, keep=True)
-    l1 = sur.backward(X, X.T.contiguous(), T).item()
+    l1 = sur.backward(X, T).item()
     torch.cuda.synchronize()
     return sur, l0, l1
 
@@ -394,7 +438,7 @@ def test_surrogate_gradient_is_smooth_across_touchdown(trained, oracle):
     w[2] = 1.0
     T = Y.clone()
     T[:, 2] -= n / 2.0  # d loss / d Y = e_2 for every row
-    sur.backward(X, X.T.contiguous(), T, want_dx=True, weights=w)
+    sur.backward(X, T, want_dx=True, weights=w)
     zi = 58  # feature index of the base height
     d_sur = (sur.dX(n)[:64, zi] * sur.in_istd[zi] * sur.out_std[2]).double().cpu().numpy()
     jump_exact = np.abs(np.diff(d_exact)).max()
