@@ -69,7 +69,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--surrogate-steps", type=int, default=3000, help="training steps of the surrogate (-1: skip)")
-    p.add_argument("--part", default="all", choices=["all", "plain", "policy", "adjoint", "gemm", "surrogate", "ppo"],
+    p.add_argument("--part", default="all", choices=["all", "plain", "policy", "adjoint", "gemm", "surrogate", "surtrain", "ppo"],
                    help="one sub-benchmark alone on --nenv envs (rows), one GPU (a small case for a profiler)")
     p.add_argument("--horizon", type=int, default=64, help="adjoint horizon with --part adjoint")
     return p.parse_args()
@@ -567,8 +567,7 @@ def surrogate_bench(device, train_steps, world):
         torch.cuda.synchronize()
         timed[name] = e0.elapsed_time(e1) / 10
     step_ms = timed["graph"]
-    macs = sum(S.DIMS[i] * S.DIMS[i + 1] for i in range(5))
-    train_tflops = 3 * 2 * SUR_BATCH * macs / (step_ms * 1e-3) / 1e12
+    train_tflops = S.train_flops(SUR_BATCH) / (step_ms * 1e-3) / 1e12
     # inference throughput of the network alone (features in HBM)
     e0.record()
     for _ in range(10):
@@ -581,7 +580,6 @@ def surrogate_bench(device, train_steps, world):
     for k in range(train_steps):
         idx = torch.randint(0, X.shape[0], (SUR_BATCH,), generator=g, device=device)
         torch.index_select(X, 0, idx, out=xb)
-        xt.copy_(xb.T)
         torch.index_select(T, 0, idx, out=tb)
         loss = tg.step(2e-3 * (0.05 ** (k / max(train_steps, 1))))
     torch.cuda.synchronize()
@@ -601,7 +599,7 @@ def surrogate_bench(device, train_steps, world):
             "train_frac_of_bf16_peak": (train_tflops / peak) if peak else None,
             "train_frac_of_bf16_sustained": (train_tflops / sustained) if sustained else None,
             "bf16_peak_tflops": peak, "bf16_peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured",
-            "train_flops_per_step": 3 * 2 * SUR_BATCH * macs,
+            "train_flops_per_step": S.train_flops(SUR_BATCH),
             "inference": {"value": SUR_BATCH / (fwd_ms * 1e-3), "unit": "env-steps/s (network forward only)"},
             "transitions": int(X.shape[0]), "generation_s": gen_s, "train_steps": train_steps,
             "loss_start": l0, "loss_end": l1,
@@ -734,6 +732,33 @@ def gemm_bench(device, rows, steps, warmup):
             "status": S.gemm_status()}
 
 
+def surtrain_bench(device, batch, steps, warmup):
+    """One surrogate training step alone (forward, loss, backward, Adam) on a
+    fixed synthetic minibatch of `batch` rows (normal BF16 features and
+    targets), replayed from its CUDA graph `steps` times after `warmup`
+    replays, timed with CUDA events."""
+    import torch
+    from g1sim_b200 import surrogate as S
+    sur = S.Surrogate(device, seed=0)
+    g = torch.Generator(device=device).manual_seed(0)
+    xb = torch.randn(batch, S.NIN, device=device, generator=g).to(torch.bfloat16)
+    tb = torch.randn(batch, 64, device=device, generator=g)
+    tg = sur.capture_train_step(xb, tb, lr=1e-3)
+    for _ in range(max(1, warmup)):
+        tg.step()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(max(1, steps)):
+        tg.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, steps)
+    return {"batch": batch, "train_step_ms": ms, "tflops": S.train_flops(batch) / (ms * 1e-3) / 1e12,
+            "loss": float(tg.loss.item()), "status": S.gemm_status()}
+
+
 def part_only(args, local):
     """One sub-benchmark alone on one GPU, printed as a diagnostic JSON line
     (not the bench line): the small cases the profiler captures run this way."""
@@ -753,6 +778,8 @@ def part_only(args, local):
         r = policy_ppo_bench(device)
     elif args.part == "surrogate":
         r = surrogate_bench(device, args.surrogate_steps, 1)
+    elif args.part == "surtrain":
+        r = surtrain_bench(device, args.nenv, args.steps, args.warmup)
     elif args.part == "adjoint":
         r = adjoint_bench(device, stream, args.steps, args.warmup, 1, n=args.nenv, horizon=args.horizon)
     else:

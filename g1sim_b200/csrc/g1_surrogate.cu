@@ -238,25 +238,28 @@ int g1b_sur_adam_cast(int nl, const g1b_sur_layer* layers, const int* step, cons
                       float eps, void* stream) {
   if (nl <= 0 || nl > kSurMaxLayers || !layers || !step || !lr) return fail("sur_adam_cast: invalid arguments");
   SurOpt o{};
-  long long total = 0;
+  long long tiles = 0, biases = 0;
   for (int i = 0; i < nl; ++i) {
     const g1b_sur_layer& L = layers[i];
     if (!L.W || !L.b || !L.mW || !L.vW || !L.mb || !L.vb || !L.gW || !L.gb || !L.Wb || !L.Wt || L.rows <= 0 ||
-        L.cols <= 0)
+        L.cols <= 0 || (long long)L.rows * L.cols > INT32_MAX)
       return fail("sur_adam_cast: invalid layer");
     o.l[i] = {L.W, L.b, L.mW, L.vW, L.mb, L.vb, L.gW, L.gb, static_cast<__nv_bfloat16*>(L.Wb),
               static_cast<__nv_bfloat16*>(L.Wt), L.rows, L.cols};
-    total += (long long)L.rows * L.cols + L.rows;
+    o.tile0[i] = (int)tiles;
+    tiles += (long long)((L.rows + kAdamRows - 1) / kAdamRows) * ((L.cols + kAdamCols - 1) / kAdamCols);
+    biases += L.rows;
   }
-  if (total > INT32_MAX) return fail("sur_adam_cast: too many parameters");
+  const long long blocks = tiles + (biases + kAdamThreads - 1) / kAdamThreads;
+  if (blocks > INT32_MAX) return fail("sur_adam_cast: too many parameters");
+  o.tile0[nl] = (int)tiles;
   o.nl = nl;
-  o.total = (int)total;
   o.step = step;
   o.lr = lr;
   o.b1 = b1;
   o.b2 = b2;
   o.eps = eps;
-  sur_adam_cast_kernel<<<grid_1d((size_t)total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(o);
+  sur_adam_cast_kernel<<<(unsigned)blocks, kAdamThreads, 0, static_cast<cudaStream_t>(stream)>>>(o);
   return launched("sur_adam_cast_kernel");
 }
 

@@ -98,8 +98,14 @@ __global__ void __launch_bounds__(kLossThreads) sur_loss_kernel(int B, int D, co
 // the step count t and the learning rate read from device memory, so that a
 // captured CUDA graph of the training step replays with the current ones),
 // then the BF16 copy and BF16 transpose of each updated weight that the
-// GEMMs read.  Thread i owns the i-th entry of the layers' weights and
-// biases taken in order.
+// GEMMs read.  Each block of kAdamThreads owns one kAdamRows x kAdamCols
+// tile of one layer's weight (row-major reads and writes, one 128-byte
+// line per warp instruction) and writes the tile's transpose from shared
+// memory as 16-byte runs of eight rows; the blocks after the last tile
+// update the biases, one entry per thread, the layers' biases in order.
+constexpr int kAdamRows = 32, kAdamCols = 64, kAdamThreads = 256;
+static_assert(kAdamCols * (kAdamRows / 8) == kAdamThreads && kAdamCols == 64 && kAdamThreads == 256,
+              "a warp's entries: 8 rows x 2 x 32 columns; one column's eight-row run per thread");
 struct SurLayerOpt {
   float *W, *b, *mW, *vW, *mb, *vb;
   const float *gW, *gb;
@@ -109,7 +115,8 @@ struct SurLayerOpt {
 constexpr int kSurMaxLayers = 8;
 struct SurOpt {
   SurLayerOpt l[kSurMaxLayers];
-  int nl, total;
+  int tile0[kSurMaxLayers + 1];  // first block of each layer's tiles; tile0[nl]: the first bias block
+  int nl;
   const int* step;
   const float* lr;
   float b1, b2, eps;
@@ -125,27 +132,71 @@ __device__ __forceinline__ float adam_update(float& p, float& m, float& v, float
   return p;
 }
 
-__global__ void sur_adam_cast_kernel(SurOpt o) {
+__global__ void __launch_bounds__(kAdamThreads) sur_adam_cast_kernel(SurOpt o) {
+  // the tile transposed: 34 values (17 words) per column, so the warps'
+  // column-wise writes fall in distinct banks
+  __shared__ __align__(16) __nv_bfloat16 tr[kAdamCols][kAdamRows + 2];
   const float t = (float)*o.step, lr = *o.lr;
   const float c1 = 1.0f - powf(o.b1, t), c2 = 1.0f - powf(o.b2, t);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.total; i += gridDim.x * blockDim.x) {
-    int k = i;
+  const int blk = blockIdx.x;
+  if (blk >= o.tile0[o.nl]) {
+    int k = (blk - o.tile0[o.nl]) * kAdamThreads + threadIdx.x;
     for (int L = 0; L < o.nl; ++L) {
       const SurLayerOpt& q = o.l[L];
-      const int nw = q.rows * q.cols;
-      if (k < nw) {
-        const float p = adam_update(q.W[k], q.mW[k], q.vW[k], q.gW[k], lr, o.b1, o.b2, o.eps, c1, c2);
-        const __nv_bfloat16 h = __float2bfloat16_rn(p);
-        q.Wb[k] = h;
-        q.Wt[(size_t)(k % q.cols) * q.rows + k / q.cols] = h;
-        break;
-      }
-      k -= nw;
       if (k < q.rows) {
         adam_update(q.b[k], q.mb[k], q.vb[k], q.gb[k], lr, o.b1, o.b2, o.eps, c1, c2);
         break;
       }
       k -= q.rows;
+    }
+    return;
+  }
+  int L = 0;
+  while (blk >= o.tile0[L + 1]) ++L;
+  const SurLayerOpt& q = o.l[L];
+  const int tcols = (q.cols + kAdamCols - 1) / kAdamCols;
+  const int r0 = ((blk - o.tile0[L]) / tcols) * kAdamRows, c0 = ((blk - o.tile0[L]) % tcols) * kAdamCols;
+  // entry e of this thread: row warp + 8 (e / 2), column lane + 32 (e % 2); every
+  // load is issued before the first store (the stores could alias the loads
+  // of a later entry, so the compiler would not hoist them by itself)
+  constexpr int kPer = kAdamRows * kAdamCols / kAdamThreads;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float w[kPer], m[kPer], v[kPer], gr[kPer];
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int r = r0 + warp + 8 * (e >> 1), c = c0 + lane + 32 * (e & 1);
+    const bool in = r < q.rows && c < q.cols;
+    const size_t k = in ? (size_t)r * q.cols + c : 0;
+    w[e] = in ? q.W[k] : 0.0f;
+    m[e] = in ? q.mW[k] : 0.0f;
+    v[e] = in ? q.vW[k] : 0.0f;
+    gr[e] = in ? q.gW[k] : 0.0f;
+  }
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int rr = warp + 8 * (e >> 1), cc = lane + 32 * (e & 1), r = r0 + rr, c = c0 + cc;
+    __nv_bfloat16 h = __float2bfloat16_rn(0.0f);
+    if (r < q.rows && c < q.cols) {
+      const size_t k = (size_t)r * q.cols + c;
+      h = __float2bfloat16_rn(adam_update(w[e], m[e], v[e], gr[e], lr, o.b1, o.b2, o.eps, c1, c2));
+      q.W[k] = w[e];
+      q.mW[k] = m[e];
+      q.vW[k] = v[e];
+      q.Wb[k] = h;
+    }
+    tr[cc][rr] = h;
+  }
+  __syncthreads();
+  const bool vec = r0 + kAdamRows <= q.rows && c0 + kAdamCols <= q.cols && (q.rows & 7) == 0 &&
+                   (reinterpret_cast<uintptr_t>(q.Wt) & 15) == 0;
+  if (vec) {  // thread: one column, eight rows
+    const int cc = threadIdx.x >> 2, j = threadIdx.x & 3;
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(&tr[cc][8 * j]);
+    *reinterpret_cast<uint4*>(q.Wt + (size_t)(c0 + cc) * q.rows + r0 + 8 * j) = make_uint4(w[0], w[1], w[2], w[3]);
+  } else {
+    for (int i = threadIdx.x; i < kAdamRows * kAdamCols; i += kAdamThreads) {
+      const int cc = i / kAdamRows, rr = i % kAdamRows;
+      if (r0 + rr < q.rows && c0 + cc < q.cols) q.Wt[(size_t)(c0 + cc) * q.rows + r0 + rr] = tr[cc][rr];
     }
   }
 }

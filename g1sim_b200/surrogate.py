@@ -43,6 +43,14 @@ DIMS = [192, 512, 512, 512, 512, 64]
 NFEAT, NOUT, NIN = 159, 35, 192
 
 
+def train_flops(batch):
+    """Floating-point operations of one training step on `batch` rows: the
+    forward products, the weight gradients, and the input gradients of every
+    layer but the first (a training step needs no d loss / d X)."""
+    macs = sum(DIMS[i] * DIMS[i + 1] for i in range(5))
+    return 2 * batch * (3 * macs - DIMS[0] * DIMS[1])
+
+
 def _p(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 

@@ -295,17 +295,53 @@ def test_adam_matches_update_rule():
         gw.normal_()
     for gb in sur.gb:
         gb.normal_()
-    g0 = [gw[:w.shape[0]].clone() for gw, w in zip(sur.gW, sur.W)]
+    b0 = [b.clone() for b in sur.b]
+    g0 = [gw.clone() for gw in sur.gW] + [gb.clone() for gb in sur.gb]
     sur.adam(lr=1e-2)
     torch.cuda.synchronize()
-    for w_new, w_old, g in zip(sur.W, w0, g0):
+    for p_new, p_old, g in zip(sur.W + sur.b, w0 + b0, g0):
         m = 0.1 * g
         v = 0.001 * g * g
-        ref = w_old - 1e-2 * (m / 0.1) / (torch.sqrt(v / 0.001) + 1e-8)
-        assert torch.allclose(w_new, ref, rtol=1e-5, atol=1e-6)
-    # BF16 copies refreshed
-    assert torch.equal(sur.Wb[0], sur.W[0].to(torch.bfloat16))
-    assert torch.equal(sur.Wt[0], sur.W[0].T.contiguous().to(torch.bfloat16))
+        ref = p_old - 1e-2 * (m / 0.1) / (torch.sqrt(v / 0.001) + 1e-8)
+        assert torch.allclose(p_new, ref, rtol=1e-5, atol=1e-6)
+    # BF16 copies and transposes of every layer refreshed
+    for i in range(5):
+        assert torch.equal(sur.Wb[i], sur.W[i].to(torch.bfloat16))
+        assert torch.equal(sur.Wt[i], sur.W[i].T.contiguous().to(torch.bfloat16))
+
+
+@pytest.mark.parametrize("shapes", [[(40, 70), (37, 5)], [(64, 128), (8, 64), (33, 200), (96, 192)]])
+def test_adam_cast_partial_tiles(shapes):
+    """The fused optimiser launch on weights that do not fill its 32 x 64
+    tiles, with row counts that are not multiples of 8 (element-wise
+    transposed stores) beside full tiles (16-byte runs), several layers and
+    their biases in one launch, against Adam's first step."""
+    g = torch.Generator(device=DEV).manual_seed(len(shapes))
+    keep, layers = [], []
+    for r, c in shapes:
+        t = dict(W=torch.randn(r, c, device=DEV, generator=g), b=torch.randn(r, device=DEV, generator=g),
+                 mW=torch.zeros(r, c, device=DEV), vW=torch.zeros(r, c, device=DEV), mb=torch.zeros(r, device=DEV),
+                 vb=torch.zeros(r, device=DEV), gW=torch.randn(r, c, device=DEV, generator=g),
+                 gb=torch.randn(r, device=DEV, generator=g), Wb=torch.empty(r, c, dtype=torch.bfloat16, device=DEV),
+                 Wt=torch.empty(c, r, dtype=torch.bfloat16, device=DEV))
+        t["W0"], t["b0"] = t["W"].clone(), t["b"].clone()
+        keep.append(t)
+        layers.append(_lib.SurLayer(*[t[k].data_ptr() for k in ("W", "b", "mW", "vW", "mb", "vb", "gW", "gb",
+                                                                 "Wb", "Wt")], r, c))
+    arr = (_lib.SurLayer * len(layers))(*layers)
+    step = torch.ones(1, dtype=torch.int32, device=DEV)
+    lr = torch.full((1,), 1e-2, device=DEV)
+    _lib.check(_lib.lib().g1b_sur_adam_cast(len(layers), arr, C.c_void_p(step.data_ptr()), C.c_void_p(lr.data_ptr()),
+                                            0.9, 0.999, 1e-8,
+                                            C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)),
+               "g1b_sur_adam_cast")
+    torch.cuda.synchronize()
+    for t in keep:
+        for p_new, p_old, gr in ((t["W"], t["W0"], t["gW"]), (t["b"], t["b0"], t["gb"])):
+            ref = p_old - 1e-2 * gr / (gr.abs() + 1e-8)  # t = 1: m / c1 = g, sqrt(v / c2) = |g|
+            assert torch.allclose(p_new, ref, rtol=1e-5, atol=1e-6)
+        assert torch.equal(t["Wb"], t["W"].to(torch.bfloat16))
+        assert torch.equal(t["Wt"], t["W"].T.contiguous().to(torch.bfloat16))
 
 
 def test_adam_bias_correction_over_steps():
@@ -318,7 +354,7 @@ def test_adam_bias_correction_over_steps():
     g = torch.Generator(device=DEV).manual_seed(5)
     for t, lr in ((1, 1e-2), (2, 5e-3), (3, 2e-3)):
         gw = torch.randn(sur.W[1].shape, device=DEV, generator=g)
-        sur.gW[1][:gw.shape[0]].copy_(gw)
+        sur.gW[1].copy_(gw)
         sur.adam(lr=lr)
         torch.cuda.synchronize()
         m = 0.9 * m + 0.1 * gw.double()
