@@ -47,10 +47,13 @@ FLOPS_EXECUTED_PER_ENV_STEP = 31385.0
 # anchor 16, ctrl 29, mu, dmass) and out (qpos, qvel, anchor, ctrl), float32.
 BYTES_PER_ENV_LAUNCH = 4.0 * ((36 + 35 + 16 + 29 + 2) + (36 + 35 + 16 + 29))
 
-# DRAM bytes per env of one split_kernel launch (10 substeps), from one ncu
-# capture at 16,384 envs (dram__bytes_read.sum + dram__bytes_write.sum =
-# 6,105,088 + 0 B; profiles/split_kernel_16384env_full.md), scaled by envs.
-NCU_DRAM_BYTES_PER_ENV_LAUNCH = 6105088.0 / 16384
+# DRAM bytes per env of the bench step's launch (split_kernel, 100 policy steps
+# = 1,000 substeps): dram__bytes_read.sum + dram__bytes_write.sum, mean of two
+# ncu captures at 16,384 envs (6,845,184 and 7,032,832 B;
+# profiles/split_kernel_65536env_launch_list.md), scaled by envs.  One
+# policy-step launch moved 6,105,088 B at 16,384 envs
+# (profiles/split_kernel_16384env_full.md).
+NCU_DRAM_BYTES_PER_ENV_PERSISTENT = 6939008.0 / 16384
 
 NENV = 65536
 SUBSTEPS = 1000
@@ -65,6 +68,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--nenv", type=int, default=NENV)
+    p.add_argument("--npolicy", type=int, default=1, help="policy steps per launch with --part plain")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
@@ -610,18 +614,18 @@ def surrogate_bench(device, train_steps, world):
             "gemm_status": S.gemm_status()}
 
 
-def plain_bench(device, n, steps, warmup):
-    """The plain step alone: one policy step (10 substeps, target redraw,
-    reset check) of n randomised envs per launch, `warmup` + `steps`
-    launches, CUDA-event timed (a small case for a profiler)."""
+def plain_bench(device, n, steps, warmup, npolicy=1):
+    """The plain step alone: `npolicy` policy steps (10 substeps, target
+    redraw, reset check each) of n randomised envs per launch, `warmup` +
+    `steps` launches, CUDA-event timed (a small case for a profiler)."""
     import torch
     from g1sim_b200 import _lib, workloads
     from g1sim_b200 import g1sim as G
     w = workloads.randomized(nenv=n, seed=0)
     st = {k: torch.tensor(w[k], dtype=torch.float32, device=device)
           for k in ("qpos", "qvel", "anchor", "ctrl", "mu", "dmass")}
-    run = lambda k: G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 1, DECIM, config=_cfg(), seed=0,  # noqa
-                              step0=k, mu=st["mu"], dmass=st["dmass"])
+    run = lambda k: G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], npolicy, DECIM,  # noqa: E731
+                              config=_cfg(), seed=0, step0=k * npolicy, mu=st["mu"], dmass=st["dmass"])
     for k in range(warmup):
         run(k)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -632,8 +636,10 @@ def plain_bench(device, n, steps, warmup):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(steps, 1)
     mapping, block, _ = _lib.get_launch()
-    return {"ms_per_launch": ms, "env_steps_per_s": n * DECIM / (ms * 1e-3),
-            "tflops": FLOPS_PER_ENV_STEP * n * DECIM / (ms * 1e-3) / 1e12, "mapping": mapping, "block": block}
+    return {"ms_per_launch": ms, "policy_steps_per_launch": npolicy,
+            "env_steps_per_s": n * DECIM * npolicy / (ms * 1e-3),
+            "tflops": FLOPS_PER_ENV_STEP * n * DECIM * npolicy / (ms * 1e-3) / 1e12, "mapping": mapping,
+            "block": block}
 
 
 def _cfg():
@@ -767,7 +773,7 @@ def part_only(args, local):
     device = torch.device("cuda", local)
     stream = torch.cuda.Stream(device)
     if args.part == "plain":
-        r = plain_bench(device, args.nenv, args.steps, args.warmup)
+        r = plain_bench(device, args.nenv, args.steps, args.warmup, args.npolicy)
     elif args.part == "policy":
         from g1sim_b200 import workloads
         w = workloads.randomized(nenv=args.nenv, seed=0)
@@ -812,28 +818,34 @@ def ours(args, world, rank, local):
     npolicy = SUBSTEPS // DECIM
     stream = torch.cuda.Stream(device)
 
-    def launch_policy_step(k):
-        G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], 1, DECIM, config=cfg, seed=rank,
-                  step0=k, mu=init["mu"], dmass=init["dmass"], reset_count=rc)
+    def launch_policy_steps(k0, count, counter):
+        G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], count, DECIM, config=cfg, seed=rank,
+                  step0=k0, mu=init["mu"], dmass=init["dmass"], reset_count=counter)
 
     def reset_state():
         for k in st:
             st[k].copy_(init[k])
 
-    # capture the 100 policy-step launches in one CUDA graph
+    # the step: one persistent launch of the 100 policy steps (each CTA keeps its envs on chip
+    # across all of them), captured in a CUDA graph; beside it the same work as a graph of 100
+    # one-policy-step launches (the state goes back to memory between policy steps)
+    rc_split = torch.zeros_like(rc)
     with torch.cuda.stream(stream):
         reset_state()
-        launch_policy_step(0)  # one eager launch before capture (kernel attributes, lazy loading)
+        launch_policy_steps(0, 1, rc_split)  # one eager launch before capture (kernel attributes, lazy loading)
         torch.cuda.synchronize()
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph, stream=stream):
+            launch_policy_steps(0, npolicy, rc)
+        graph_split = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph_split, stream=stream):
             for k in range(npolicy):
-                launch_policy_step(k)
-    launches_per_step = npolicy
+                launch_policy_steps(k, 1, rc_split)
+    launches_per_step = 1
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > 126 MB L2
 
-    def timed_steps(count):
+    def timed_steps(count, g):
         times = []
         for _ in range(count):
             with torch.cuda.stream(stream):
@@ -842,18 +854,18 @@ def ours(args, world, rank, local):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                graph.replay()
+                g.replay()
                 e1.record(stream)
             stream.synchronize()
             times.append(e0.elapsed_time(e1))
         return times
 
-    timed_steps(args.warmup)
+    timed_steps(args.warmup, graph)
     barrier(world)
     torch.cuda.synchronize()
     rc0 = int(rc.sum().item())
     with ClockSampler(local) as clk:
-        times = timed_steps(args.steps)
+        times = timed_steps(args.steps, graph)
     torch.cuda.synchronize()
     barrier(world)
     resets_per_step = (int(rc.sum().item()) - rc0) / max(args.steps, 1)
@@ -861,10 +873,13 @@ def ours(args, world, rank, local):
     ms = max_over_ranks(statistics.mean(times), world, device)
     env_steps = float(n) * SUBSTEPS
     value = env_steps * world / (ms * 1e-3)
+    # the same work as 100 one-policy-step launches (same warm-up and timing), reported alongside
+    timed_steps(args.warmup, graph_split)
+    ms_split = max_over_ranks(statistics.mean(timed_steps(args.steps, graph_split)), world, device)
 
-    # ---- kernel-level roofline (dominant kernel: one policy-step launch)
+    # ---- kernel-level roofline (dominant kernel: the persistent launch of 100 policy steps)
     launch_ms = ms / launches_per_step
-    flops_launch = FLOPS_PER_ENV_STEP * n * DECIM
+    flops_launch = FLOPS_PER_ENV_STEP * n * SUBSTEPS
     achieved_tf = flops_launch / (launch_ms * 1e-3) / 1e12
     ffma_tf = C.c_float()
     ffma_ms = C.c_float()
@@ -872,20 +887,8 @@ def ours(args, world, rank, local):
     peak_tf = float(ffma_tf.value)
     hbm_gbs = BYTES_PER_ENV_LAUNCH * n / (launch_ms * 1e-3) / 1e9
     mapping, block, _ = _lib.get_launch()
-    kernel_name = (f"split_kernel<{block}, rollout> (2 threads per env), 1 policy step" if mapping == 1
-                   else f"rollout_kernel<{block}> (1 thread per env), 1 policy step")
-
-    # ---- single-launch (fully persistent) variant, reported alongside
-    with torch.cuda.stream(stream):
-        reset_state()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        G.rollout(st["qpos"], st["qvel"], st["anchor"], st["ctrl"], npolicy, DECIM, config=cfg, seed=rank,
-                  step0=0, mu=init["mu"], dmass=init["dmass"], reset_count=rc)
-        e1.record(stream)
-    stream.synchronize()
-    single_ms = e0.elapsed_time(e1)
+    kernel_name = (f"split_kernel<{block}, rollout> (2 threads per env), {npolicy} policy steps per launch"
+                   if mapping == 1 else f"rollout_kernel<{block}> (1 thread per env), {npolicy} policy steps per launch")
 
     # ---- end to end through the public API, host buffers in pinned memory
     host_in = {k: init[k].cpu().pin_memory() for k in init}
@@ -898,9 +901,8 @@ def ours(args, world, rank, local):
         with torch.cuda.stream(stream):
             for k in host_in:
                 dev_in[k].copy_(host_in[k], non_blocking=True)
-            for k in range(npolicy):
-                G.rollout(dev_in["qpos"], dev_in["qvel"], dev_in["anchor"], dev_in["ctrl"], 1, DECIM, config=cfg,
-                          seed=rank, step0=k, mu=dev_in["mu"], dmass=dev_in["dmass"])
+            G.rollout(dev_in["qpos"], dev_in["qvel"], dev_in["anchor"], dev_in["ctrl"], npolicy, DECIM, config=cfg,
+                      seed=rank, step0=0, mu=dev_in["mu"], dmass=dev_in["dmass"])
             for k in host_out:
                 host_out[k].copy_(dev_in[k], non_blocking=True)
         stream.synchronize()
@@ -934,13 +936,15 @@ def ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"randomised plain step, {n} envs per GPU, dt 2 ms, decimation 10, "
-                                   f"{SUBSTEPS} substeps per step (CUDA graph of {npolicy} policy-step launches)",
+                                   f"{SUBSTEPS} substeps per step (one persistent launch of {npolicy} policy steps, "
+                                   f"in a CUDA graph)",
                        "envs_per_gpu": n, "substeps": SUBSTEPS, "decimation": DECIM, "dt": DT,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
             "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                          "frac": achieved_tf / peak_tf if peak_tf > 0 else None,
-                         "traffic": NCU_DRAM_BYTES_PER_ENV_LAUNCH * n,
-                         "traffic_source": "ncu DRAM bytes of one split_kernel launch at 16,384 envs, scaled by envs",
+                         "traffic": NCU_DRAM_BYTES_PER_ENV_PERSISTENT * n,
+                         "traffic_source": f"ncu DRAM bytes of one split_kernel launch of {npolicy} policy steps at "
+                                           f"16,384 envs, scaled by envs",
                          "algorithmic_bytes": BYTES_PER_ENV_LAUNCH * n,
                          "peak_source": "measured FFMA microbenchmark (g1b_ffma_peak), this run",
                          "flops_per_env_step": FLOPS_PER_ENV_STEP,
@@ -952,7 +956,8 @@ def ours(args, world, rank, local):
             "e2e": {"value": e2e_value, "unit": "env-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
-            "single_launch": {"value": env_steps / (single_ms * 1e-3), "ms": single_ms},
+            "per_policy_step_launches": {"value": env_steps * world / (ms_split * 1e-3), "ms": ms_split,
+                                         "form": f"CUDA graph of {npolicy} one-policy-step launches"},
             "resets_per_timed_step": resets_per_step, "finite": finite, "accuracy": accuracy,
             "policy_fused": pol,
             "policy_ppo": ppo,
