@@ -35,24 +35,24 @@ __global__ void __launch_bounds__(kLossThreads) sur_loss_kernel(int B, int D, co
   const int r0 = blockIdx.x * kLossRows;
   const int rows = B - r0 < kLossRows ? B - r0 : kLossRows;
   const int ld = D + 2;
-  const int c = threadIdx.x % D;
+  // the thread's column is fixed (D divides the block) and its rows step by
+  // kLossThreads / D: row r_t, r_t + rpp, ...
+  const int c = threadIdx.x % D, r_t = threadIdx.x / D, rpp = kLossThreads / D;
   const float wc = w[c];
-  const int total = rows * D;
   float acc = 0.0f, l = 0.0f;
   // eight rows' loads in flight per thread before their arithmetic
-  for (int i0 = threadIdx.x; i0 < total; i0 += 8 * kLossThreads) {
+  for (int rb = r_t; rb < rows; rb += 8 * rpp) {
     float e[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int i = i0 + u * kLossThreads;
-      const size_t gi = (size_t)(r0 + i / D) * D + c;
-      e[u] = i < total ? Y[gi] - T[gi] : 0.0f;
+      const int r = rb + u * rpp;
+      const size_t gi = (size_t)(r0 + r) * D + c;
+      e[u] = r < rows ? Y[gi] - T[gi] : 0.0f;
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int i = i0 + u * kLossThreads;
-      if (i >= total) continue;
-      const int r = i / D;
+      const int r = rb + u * rpp;
+      if (r >= rows) continue;
       l += wc * e[u] * e[u];
       const float g = 2.0f * wc * e[u] / (float)B;
       acc += g;

@@ -164,10 +164,11 @@ def test_linear_silu_fused_epilogue(M_, N, K):
     assert torch.equal(H2, H)
 
 
-@pytest.mark.parametrize("M_,N,K", [(256, 512, 512), (20480, 512, 512), (384, 192, 512), (128, 48, 64)])
+@pytest.mark.parametrize("M_,N,K", [(256, 512, 512), (20480, 512, 512), (384, 192, 512), (128, 48, 64),
+                                    (256, 768, 256)])
 def test_linear_silu_bwd_fused_epilogue(M_, N, K):
     """g = (dZ Wt^T) * silu'(Z), dH = bf16(g), dHt = dH^T, db += column sums of
-    g in one kernel, against FP64."""
+    g in one kernel, against FP64 (N = 768: three column tiles)."""
     g = torch.Generator(device=DEV).manual_seed(5 * M_ + N)
     dZ = bf(torch.randn(M_, K, device=DEV, generator=g))
     Wt = bf(torch.randn(N, K, device=DEV, generator=g) / K ** 0.5)
