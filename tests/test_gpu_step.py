@@ -187,9 +187,12 @@ def test_rollout_targets_bit_exact_and_parity(oracle, shape):
     assert resets_gpu > 0
 
 
-def test_rollout_is_deterministic_and_composes(shape):
-    """rollout(npolicy=4) == 4 x rollout(npolicy=1, step0=k), bit for bit."""
-    n = 300
+@pytest.mark.parametrize("n", [300, 40000])
+def test_rollout_is_deterministic_and_composes(n, shape):
+    """rollout(npolicy=4) == 4 x rollout(npolicy=1, step0=k), bit for bit:
+    one tile per CTA (300 envs) and several tiles per CTA, the last one
+    ragged (40,000 envs: 313 tiles of 128), the persistent form of the
+    bench step."""
     w = workloads.randomized(nenv=n, seed=2)
     a = [dev(w[k]) for k in ("qpos", "qvel", "anchor", "ctrl")]
     b = [t.clone() for t in a]
