@@ -73,7 +73,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--surrogate-steps", type=int, default=3000, help="training steps of the surrogate (-1: skip)")
-    p.add_argument("--part", default="all", choices=["all", "plain", "policy", "adjoint", "gemm", "surrogate", "surtrain", "ppo"],
+    p.add_argument("--part", default="all",
+                   choices=["all", "plain", "policy", "adjoint", "gemm", "surrogate", "surtrain", "ppo"],
                    help="one sub-benchmark alone on --nenv envs (rows), one GPU (a small case for a profiler)")
     p.add_argument("--horizon", type=int, default=64, help="adjoint horizon with --part adjoint")
     return p.parse_args()
@@ -887,8 +888,8 @@ def ours(args, world, rank, local):
     peak_tf = float(ffma_tf.value)
     hbm_gbs = BYTES_PER_ENV_LAUNCH * n / (launch_ms * 1e-3) / 1e9
     mapping, block, _ = _lib.get_launch()
-    kernel_name = (f"split_kernel<{block}, rollout> (2 threads per env), {npolicy} policy steps per launch"
-                   if mapping == 1 else f"rollout_kernel<{block}> (1 thread per env), {npolicy} policy steps per launch")
+    kernel_name = (f"split_kernel<{block}, rollout> (2 threads per env)" if mapping == 1
+                   else f"rollout_kernel<{block}> (1 thread per env)") + f", {npolicy} policy steps per launch"
 
     # ---- end to end through the public API, host buffers in pinned memory
     host_in = {k: init[k].cpu().pin_memory() for k in init}
