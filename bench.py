@@ -888,8 +888,10 @@ def ours(args, world, rank, local):
     peak_tf = float(ffma_tf.value)
     hbm_gbs = BYTES_PER_ENV_LAUNCH * n / (launch_ms * 1e-3) / 1e9
     mapping, block, _ = _lib.get_launch()
-    kernel_name = (f"split_kernel<{block}, rollout> (2 threads per env)" if mapping == 1
-                   else f"rollout_kernel<{block}> (1 thread per env)") + f", {npolicy} policy steps per launch"
+    kernel_name = {0: f"rollout_kernel<{block}> (1 thread per env)",
+                   1: f"split_kernel<{block}, rollout> (2 threads per env)",
+                   2: f"split3_kernel<{block}, rollout> (3 threads per env)"}.get(mapping, "?") + \
+        f", {npolicy} policy steps per launch"
 
     # ---- end to end through the public API, host buffers in pinned memory
     host_in = {k: init[k].cpu().pin_memory() for k in init}
