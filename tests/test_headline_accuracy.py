@@ -11,7 +11,11 @@ checked against the FP64 oracle:
     qvel within 1e-5 (median 1e-6) -- the metric's 1e-5 bound per step;
   * one decimated policy step (target redraw, 10 compounded substeps, reset
     check) against the oracle's rollout from the same state: the compounded
-    error stays at the per-step level times the substeps.
+    error stays at the per-step level times the substeps.  Envs whose oracle
+    trajectory comes within rounding distance of a branch (contact switch,
+    stick / slip, clamps, soft limits) at any of the 10 substeps are left
+    out: there two FP32 builds that round differently in the last bit may
+    take different sides of the switch.
 """
 import numpy as np
 import pytest
@@ -73,11 +77,18 @@ def test_policy_step_parity_all_envs(oracle, mid_rollout):
     st, mu, dm, w = mid_rollout
     s = {k: v.clone() for k, v in st.items()}
     q64, v64, a64, c64 = (host(s[k]) for k in ("qpos", "qvel", "anchor", "ctrl"))
+    qt, vt, at = q64.copy(), v64.copy(), a64.copy()
+    mu64, dm64 = w["mu"].astype(np.float64), w["dmass"].astype(np.float64)
+    cfg64 = oracle.config(dt=2e-3)
     rc64 = np.zeros(N, dtype=np.int32)
-    margin = oracle.branch_margin(oracle.config(dt=2e-3), q64, v64, a64, c64, mu=w["mu"].astype(np.float64),
-                                  dmass=w["dmass"].astype(np.float64))
-    oracle.rollout_soa(1, 10, oracle.config(dt=2e-3), RolloutParams(0, 20, 0.3, 0.3, 0.75, 0.85, 1), q64, v64, a64,
-                       c64, mu=w["mu"].astype(np.float64), dmass=w["dmass"].astype(np.float64), reset_count=rc64)
+    oracle.rollout_soa(1, 10, cfg64, RolloutParams(0, 20, 0.3, 0.3, 0.75, 0.85, 1), q64, v64, a64, c64,
+                       mu=mu64, dmass=dm64, reset_count=rc64)
+    # branch distance along the oracle's trajectory through the policy step (the redrawn targets
+    # c64 held for its substeps; for envs that do not reset it is the rollout's trajectory)
+    margin = np.full(N, np.inf)
+    for _ in range(10):
+        margin = np.minimum(margin, oracle.branch_margin(cfg64, qt, vt, at, c64, mu=mu64, dmass=dm64))
+        oracle.step_soa(1, cfg64, qt, vt, at, c64, mu=mu64, dmass=dm64, outputs=False)
     rc = torch.zeros(N, dtype=torch.int32, device=DEV)
     G.rollout(s["qpos"], s["qvel"], s["anchor"], s["ctrl"], 1, 10, seed=0, step0=20, mu=mu, dmass=dm, reset_count=rc)
     torch.cuda.synchronize()
