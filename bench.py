@@ -49,11 +49,11 @@ BYTES_PER_ENV_LAUNCH = 4.0 * ((36 + 35 + 16 + 29 + 2) + (36 + 35 + 16 + 29))
 
 # DRAM bytes per env of the bench step's launch (split_kernel, 100 policy steps
 # = 1,000 substeps): dram__bytes_read.sum + dram__bytes_write.sum, mean of two
-# ncu captures at 16,384 envs (6,845,184 and 7,032,832 B;
+# ncu captures at 16,384 envs (6,554,880 and 6,892,032 B;
 # profiles/split_kernel_65536env_launch_list.md), scaled by envs.  One
 # policy-step launch moved 6,105,088 B at 16,384 envs
 # (profiles/split_kernel_16384env_full.md).
-NCU_DRAM_BYTES_PER_ENV_PERSISTENT = 6939008.0 / 16384
+NCU_DRAM_BYTES_PER_ENV_PERSISTENT = 6723456.0 / 16384
 
 NENV = 65536
 SUBSTEPS = 1000

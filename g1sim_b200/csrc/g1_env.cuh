@@ -28,7 +28,7 @@ struct SmemScratch {
 template <int BLOCK>
 constexpr size_t smem_bytes() { return (size_t)kNumSlotsSingle * BLOCK * sizeof(float); }
 template <int ENVS>
-constexpr size_t smem_bytes_split() { return (size_t)kNumSlots * ENVS * sizeof(float); }
+constexpr size_t smem_bytes_split() { return (size_t)kNumSlotsSplit * ENVS * sizeof(float); }
 
 struct StateArgs {
   int nenv;
@@ -81,6 +81,7 @@ __device__ __forceinline__ EnvIO env_io(const StateArgs& a, const float* ctrl, i
   io.foot_vel = a.foot_vel ? a.foot_vel + e : nullptr;
   io.cf = a.cf ? a.cf + e : nullptr;
   io.stride = (size_t)a.nenv;
+  io.astride = (size_t)a.nenv;
   return io;
 }
 

@@ -455,6 +455,12 @@ constexpr int kNumSlots = kSlotXchg + 47;   // two threads per env
 // leg's projection into the pelvis (27)
 constexpr int kXLeg = kNumSlots;
 constexpr int kNumSlots3 = kNumSlots + 27;
+// two threads per env: the env's contact anchors (2 per sphere), held on chip
+// for every substep of a tile instead of read from and written to global
+// memory in each one (a re-read after the previous substep's store is not an
+// L1 hit, and the contacts wait on it)
+constexpr int kXAnchor = kNumSlots;
+constexpr int kNumSlotsSplit = kNumSlots + 2 * kNC;
 constexpr int kSlotJointState = 2 * kNJ;  // q and qd of every hinge
 G1_CE int hslot(int body, int k) {
   return k < 2 ? k * kNJ + (body - 1) : kSlotJointState + (body - 1) * (kSlotsPerHinge - 2) + (k - 2);
@@ -470,11 +476,12 @@ struct EnvState {
 // and written by the contacts, last-substep outputs (nullable).
 struct EnvIO {
   const float* ctrl;
-  float* anchor;
+  float* anchor;  // element i at anchor[i * astride]
   float* foot_pos;
   float* foot_vel;
   float* cf;
   size_t stride;
+  size_t astride;
 };
 struct EnvParams {
   float mu, dmass, kp_scale, kd_scale;
@@ -614,7 +621,7 @@ G1_HD void fk_chain(int first, int last, FKNode& n, Scr& scr) {
 // frame once; returns the wrench's contribution to the foot's bias force.
 G1_HD SV foot_contacts(int K0, const FKNode& n, const EnvIO& io, bool last, const StepConfig& cfg, float mu) {
   float* anchor = io.anchor;
-  const size_t sd = io.stride;
+  const size_t sd = io.stride, sa = io.astride;
   const V3 ww = mv(n.R, n.w);  // world angular velocity
   const V3 vo = mv(n.R, n.v);  // world velocity of the foot origin
   V3 F = mk3(0.f, 0.f, 0.f), Tq = mk3(0.f, 0.f, 0.f);
@@ -637,7 +644,7 @@ G1_HD SV foot_contacts(int K0, const FKNode& n, const EnvIO& io, bool last, cons
     const V3 vp = add(vo, crs(ww, rw));
     float fn = cfg.contact_kn * depth - cfg.contact_dn * vp.v[2];
     fn = fminf(fmaxf(fn, 0.0f), 500.0f);
-    float ax = anchor[(2 * k) * sd], ay = anchor[(2 * k + 1) * sd];
+    float ax = anchor[(2 * k) * sa], ay = anchor[(2 * k + 1) * sa];
     const bool fresh = ax >= kAnchorFree;
     ax = fresh ? px : ax;
     ay = fresh ? py : ay;
@@ -654,15 +661,15 @@ G1_HD SV foot_contacts(int K0, const FKNode& n, const EnvIO& io, bool last, cons
       ay = py + (fty * inv_kt + pc[1].lo);
     }
     if (in) {
-      anchor[(2 * k) * sd] = ax;
-      anchor[(2 * k + 1) * sd] = ay;
+      anchor[(2 * k) * sa] = ax;
+      anchor[(2 * k + 1) * sa] = ay;
       const V3 f = mk3(ftx, fty, fn);
       F = add(F, f);
       Tq = add(Tq, crs(rw, f));
     } else {
       fn = 0.0f;
-      anchor[(2 * k) * sd] = kAnchorFree;
-      anchor[(2 * k + 1) * sd] = kAnchorFree;
+      anchor[(2 * k) * sa] = kAnchorFree;
+      anchor[(2 * k + 1) * sa] = kAnchorFree;
     }
     if (last && io.cf) io.cf[k * sd] = fn;
   }

@@ -115,6 +115,12 @@ __global__ void __launch_bounds__(2 * ENVS) split_kernel(StateArgs a, float* ctr
         for (int k = 0; k < 3; ++k) st.wb[k] = a.qvel[(3 + k) * sd + e];
         load_joints(a.qpos + e, a.qvel + e, sd, scr, 1, 12);
         store_base(scr, st);
+        // the contacts (this role) use the anchors on chip for the whole tile
+        float* an = scr.p + kXAnchor * ENVS;
+#pragma unroll
+        for (int i = 0; i < 2 * kNC; ++i) an[i * ENVS] = a.anchor[(size_t)i * sd + e];
+        io.anchor = an;
+        io.astride = ENVS;
       } else {
         load_joints(a.qpos + e, a.qvel + e, sd, scr, 13, kNJ);
       }
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(2 * ENVS) split_kernel(StateArgs a, float* ctr
               scr.put(hslot(i, 1), 0.0f);
             }
 #pragma unroll
-            for (int i = 0; i < 2 * kNC; ++i) a.anchor[(size_t)i * sd + e] = kAnchorFree;
+            for (int i = 0; i < 2 * kNC; ++i) io.anchor[i * io.astride] = kAnchorFree;
             store_base(scr, st);
             ++resets;
           }
@@ -212,6 +218,8 @@ __global__ void __launch_bounds__(2 * ENVS) split_kernel(StateArgs a, float* ctr
 #pragma unroll
         for (int k = 0; k < 3; ++k) a.qvel[(3 + k) * sd + e] = st.wb[k];
         store_joints(a.qpos + e, a.qvel + e, sd, scr, 1, 12);
+#pragma unroll
+        for (int i = 0; i < 2 * kNC; ++i) a.anchor[(size_t)i * sd + e] = io.anchor[i * ENVS];
         if (kRollout && reset_count) reset_count[e] += resets;
       } else {
         store_joints(a.qpos + e, a.qvel + e, sd, scr, 13, kNJ);
