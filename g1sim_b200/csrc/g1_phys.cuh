@@ -457,8 +457,8 @@ constexpr int kXLeg = kNumSlots;
 constexpr int kNumSlots3 = kNumSlots + 27;
 // two threads per env: the env's contact anchors (2 per sphere), held on chip
 // for every substep of a tile instead of read from and written to global
-// memory in each one (a re-read after the previous substep's store is not an
-// L1 hit, and the contacts wait on it)
+// memory in each one (the contacts waited on those reads, each right after
+// the previous substep's store)
 constexpr int kXAnchor = kNumSlots;
 constexpr int kNumSlotsSplit = kNumSlots + 2 * kNC;
 constexpr int kSlotJointState = 2 * kNJ;  // q and qd of every hinge
