@@ -50,6 +50,8 @@ constexpr size_t kPolicyScratch = (size_t)kNumSlots * kPolicyEnvs * sizeof(float
 constexpr size_t kPolicyRingEnd = (size_t)kPolicyStageOff + (size_t)tc::kStages * tc::kStageBytes;
 constexpr size_t kPolicySmem = kPolicyScratch > kPolicyRingEnd ? kPolicyScratch : kPolicyRingEnd;
 static_assert(kPolicySmem + 4096 <= 232448, "dynamic + static shared memory must fit one CTA");
+static_assert((size_t)kNumSlotsSplit * kPolicyEnvs * sizeof(float) <= kPolicySmem,
+              "the physics' anchor slots lie inside the allocation");
 static_assert(kPolicyActOff % 16 == 0 && kPolicyStageOff % 16 == 0, "operand tiles need 16-byte alignment");
 
 enum : int { kFlagSample = 1, kFlagPush = 2, kFlagReset = 4, kFlagCommands = 8 };
@@ -396,6 +398,17 @@ __device__ bool policy_pass(tc::Pipe& p, PolicyShared& ps, uint8_t* smraw, int r
 __device__ __noinline__ EnvState policy_substeps(int role, bool act, EnvState st, EnvIO io, EnvParams ep,
                                                  StepConfig cfg, float* col, int decim) {
   SmemScratch<kPolicyEnvs> scr{col};
+  // the contacts' anchors on chip for these substeps (the network phase's
+  // weight ring holds their slots in between): loaded here, stored at the end
+  float* const gan = io.anchor;
+  const size_t gsd = io.astride;
+  if (act && role == 0) {
+    float* an = scr.p + kXAnchor * kPolicyEnvs;
+#pragma unroll
+    for (int i = 0; i < 2 * kNC; ++i) an[i * kPolicyEnvs] = gan[i * gsd];
+    io.anchor = an;
+    io.astride = kPolicyEnvs;
+  }
   for (int s = 0; s < decim; ++s) {
     const bool last_sub = s == decim - 1;
     AI acc0;
@@ -432,6 +445,10 @@ __device__ __noinline__ EnvState policy_substeps(int role, bool act, EnvState st
       if (role == 0) store_base(scr, st);
     }
     __syncthreads();
+  }
+  if (act && role == 0) {
+#pragma unroll
+    for (int i = 0; i < 2 * kNC; ++i) gan[i * gsd] = io.anchor[i * kPolicyEnvs];
   }
   return st;
 }
